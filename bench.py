@@ -1,0 +1,385 @@
+"""Benchmark of the plain k-clique counting path (4-clique and 5-clique) on the citation-graph
+shaped workload: R-MAT scale 22 (4,194,304 vertices), edge factor 4, a/b/c/d =
+0.57/0.19/0.19/0.05, seed 1, degree-oriented DAG resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl jgpm|reference]
+
+A step is one exact 4-clique count plus one exact 5-clique count of the whole graph, each a
+plain single-query call of the library.  The metric is set-op elements per second: the
+set-op operand elements of the canonical edge-rooted plan (every level-1 arc intersection
+N+(u) & N+(v) adds d+(u)+d+(v), every deeper "W & N+(v)" adds |W|+d+(v)), counted exactly
+by the library's accounting pass and cross-checked against the oracle in the tests.
+Between timed steps L2 is flushed by writing a 512 MiB buffer (the graph is ~100 MB, below
+the 126 MB L2).  Multi-GPU (torchrun): every rank holds a replica and counts the full
+workload (weak scaling, replicas); the counts are summed with one NCCL all-reduce.
+
+The reference arm (--impl reference) times the reference's own host code (its AVX2
+set-intersection and graph loader, compiled from its sources into oracle/_ref/) driving the
+same plans on all host cores, over a bounded sample of root arcs of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {"workload": "k-clique (k=4,5) on R-MAT scale 22, edge factor 4, "
+                        "a/b/c/d=0.57/0.19/0.19/0.05, seed 1, degree-oriented DAG",
+            "scale": 22, "edge_factor": 4, "a": 0.57, "b": 0.19, "c": 0.19, "seed": 1,
+            "patterns": ["4-clique", "5-clique"], "l2": "flushed between steps (512 MiB write)"}
+METRIC = "matches/s + set-op elems/s (% HBM roofline); served vs plain queries/s, p50/p99"
+UNIT = "set-op elems/s"
+N_VERT = 1 << 22
+EDGE_FACTOR = 4
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), \
+        int(os.environ.get("WORLD_SIZE", 1))
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_jgpm(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import jupiter_b200 as J
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    J.lib().jgpm_set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    g = J.Graph.rmat(N_VERT, EDGE_FACTOR, 0.57, 0.19, 0.19, 1, use_dag=True)
+    info = g.info()
+    stream = torch.cuda.ExternalStream(g.stream(), device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+
+    # untimed: exact counts and the canonical plan's set-op elements
+    c4, st4 = g.count("4-clique", stats=True)
+    c5, st5 = g.count("5-clique", stats=True)
+    elems4, elems5 = st4["setop_elements"], st5["setop_elements"]
+    elems_step = elems4 + elems5
+    matches_step = c4 + c5
+
+    def step(events):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e2 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        a, sa = g.count("4-clique", details=True)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        b, sb = g.count("5-clique", details=True)
+        with torch.cuda.stream(stream):
+            e2.record(stream)
+        if a != c4 or b != c5:
+            raise RuntimeError(f"count changed between runs: {a} {b} vs {c4} {c5}")
+        events.append((e0, e1, e2, sa["launches"] + sb["launches"]))
+
+    for _ in range(args.warmup):
+        step([])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    events = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            step(events)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t4 = [e0.elapsed_time(e1) for e0, e1, e2, _ in events]
+    t5 = [e1.elapsed_time(e2) for e0, e1, e2, _ in events]
+    step_ms = [a + b for a, b in zip(t4, t5)]
+    total_ms = sum(step_ms)
+    launches = sum(x[3] for x in events)
+    if world > 1:
+        tt = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        cnt = torch.tensor([matches_step], dtype=torch.int64, device=dev)
+        dist.all_reduce(cnt)  # the one exchange: sum of the replicas' counts
+        if int(cnt.item()) != world * matches_step:
+            raise RuntimeError("replica counts disagree")
+    ms_per_step = total_ms / args.steps
+    value = world * elems_step / (ms_per_step / 1e3)
+
+    # e2e: through the public API with host buffers (pinned), H2D + orientation + both
+    # counts + the result read-back inside the timed region
+    rowptr, col = g.csr()
+    h_rowptr = torch.from_numpy(rowptr).pin_memory()
+    h_col = torch.from_numpy(col).pin_memory()
+    P64 = ctypes.POINTER(ctypes.c_int64)
+    P32 = ctypes.POINTER(ctypes.c_int32)
+    rp_ptr = ctypes.cast(h_rowptr.data_ptr(), P64)
+    col_ptr = ctypes.cast(h_col.data_ptr(), P32)
+
+    def e2e_step():
+        h = ctypes.c_void_p()
+        rc = J.lib().jgpm_graph_from_csr(rp_ptr, col_ptr, len(rowptr) - 1, len(col), 1,
+                                         ctypes.byref(h))
+        if rc:
+            raise RuntimeError(J.lib().jgpm_last_error().decode())
+        gg = J.Graph(h.value)
+        a = gg.count("4-clique")
+        b = gg.count("5-clique")
+        gg.close()
+        if a != c4 or b != c5:
+            raise RuntimeError("e2e count mismatch")
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    if world > 1:
+        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    h2d = rowptr.nbytes + col.nbytes
+    d2h = 2 * 8
+
+    peak, peak_kind = peaks()
+    k4_ms = sum(t4) / len(t4)
+    achieved = 4.0 * elems4 / (k4_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get("4-clique_bytes_per_launch")
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded R-MAT stands in for the absent citation dataset)",
+        "config": dict(WORKLOAD, parallelism=f"replicas{world}" if world > 1 else "single",
+                       num_vertices=info["num_vertices"], num_arcs=info["num_arcs"],
+                       num_dag_arcs=info["num_dag_arcs"],
+                       max_out_degree=info["max_out_degree"]),
+        "matches_per_s": world * matches_step / (ms_per_step / 1e3),
+        "counts": {"4-clique": c4, "5-clique": c5},
+        "setop_elements": {"4-clique": elems4, "5-clique": elems5},
+        "ms": {"4-clique": k4_ms, "5-clique": sum(t5) / len(t5)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "4-clique count (bitmap clique tiers)", "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": 4 * elems4},
+        "e2e": {"value": world * elems_step / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    g.close()
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ------------------------------------------------------------------ CPU reference / baseline
+def _cpu_graph():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    g = O.rmat_graph(N_VERT, EDGE_FACTOR, 0.57, 0.19, 0.19, 1)
+    return O, g
+
+
+def _sample_stride(total_arcs, target_arcs):
+    return max(1, total_arcs // max(1, target_arcs))
+
+
+def cpu_baseline(seconds=15.0, O=None, g=None, rg=None):
+    """The reference's host code (oracle/_ref) on a strided sample of root arcs, all cores."""
+    if O is None:
+        O, g = _cpu_graph()
+    dag = O.orient(g)
+    threads = os.cpu_count() or 1
+    tmp = None
+    if rg is None:
+        tmp = tempfile.TemporaryDirectory()
+        prefix = os.path.join(tmp.name, "g")
+        O.write_reference_files(g, prefix)
+        rg = O.RefGraph(prefix, use_dag=True)
+    # calibrate the stride so the sample runs ~`seconds`
+    stride = _sample_stride(dag.m, 20000)
+    c, t = rg.count("P13", 0, dag.m, stride, threads)
+    c5, t5 = rg.count("P14", 0, dag.m, stride, threads)
+    per = (t + t5) / max(1, (dag.m + stride - 1) // stride)
+    want = max(1, int(seconds / max(per, 1e-9)))
+    stride = max(1, dag.m // want)
+    c, t = rg.count("P13", 0, dag.m, stride, threads)
+    c5, t5 = rg.count("P14", 0, dag.m, stride, threads)
+    _, e4 = O.count("P13", dag, 0, dag.m, stride, threads)
+    _, e5 = O.count("P14", dag, 0, dag.m, stride, threads)
+    if tmp is not None:
+        rg.close()
+        tmp.cleanup()
+    return {"value": (e4 + e5) / (t + t5), "unit": UNIT, "cores": threads,
+            "kind": "reference", "seconds": t + t5,
+            "sample": f"every {stride}th root arc of the DAG ({(dag.m + stride - 1) // stride} of "
+                      f"{dag.m}), 4-clique + 5-clique plans over the reference's AVX2 "
+                      f"SetIntersection (common/intersect.cc)",
+            "cpu": _cpu_model()}
+
+
+def _cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    O, g = _cpu_graph()
+    dag = O.orient(g)
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = os.path.join(tmp, "g")
+        O.write_reference_files(g, prefix)
+        rg = O.RefGraph(prefix, use_dag=True)
+        threads = os.cpu_count() or 1
+        per_step = max(1.0, args.cpu_seconds / max(1, args.steps + args.warmup))
+        stride = _sample_stride(dag.m, 20000)
+        _, t4 = rg.count("P13", 0, dag.m, stride, threads)
+        _, t5 = rg.count("P14", 0, dag.m, stride, threads)
+        per = (t4 + t5) / max(1, (dag.m + stride - 1) // stride)
+        stride = max(1, dag.m // max(1, int(per_step / max(per, 1e-9))))
+        _, e4 = O.count("P13", dag, 0, dag.m, stride, threads)
+        _, e5 = O.count("P14", dag, 0, dag.m, stride, threads)
+        for _ in range(args.warmup):
+            rg.count("P13", 0, dag.m, stride, threads)
+            rg.count("P14", 0, dag.m, stride, threads)
+        secs = 0.0
+        for i in range(args.steps):
+            off = i % stride
+            _, a = rg.count("P13", off, dag.m, stride, threads)
+            _, b = rg.count("P14", off, dag.m, stride, threads)
+            secs += a + b
+        rg.close()
+    ms_per_step = secs * 1e3 / args.steps
+    value = (e4 + e5) / (ms_per_step / 1e3)
+    sample = (f"every {stride}th root arc of the DAG per step (offset varies by step), "
+              f"4-clique + 5-clique plans over the reference's AVX2 SetIntersection")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+           "data": "synthetic (seeded R-MAT stands in for the absent citation dataset)",
+           "config": dict(WORKLOAD, parallelism="host cores"),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                            "sample": sample, "cpu": _cpu_model()},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="jgpm", choices=["jgpm", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_jgpm(args)
+
+
+if __name__ == "__main__":
+    main()

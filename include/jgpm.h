@@ -1,0 +1,186 @@
+/*
+ * jgpm.h -- C-ABI of libjgpm, the B200 subgraph-pattern counting library.
+ *
+ * Plain C types only: pointers, sizes and status codes; no CUDA or torch types cross this
+ * boundary.  Every entry point returns JGPM_OK (0) or a negative JGPM_E* status and never
+ * calls exit(); jgpm_last_error() gives the message of the calling thread's last failure.
+ * The library owns the device memory it allocates; callers own their host arrays.  A graph
+ * handle may be used by one host thread at a time.
+ *
+ * Reference interfaces replaced (paths inside the AnySparse/Jupiter tree) are cited per entry
+ * point.  The reference exposes no plugin API or FFI of its own; its operator surface is
+ * the CLI `jupiter_gpm <graph_prefix> <pattern> [rounds]` (src/main.cc:7-47), the solver
+ * SubgraphSolver(Graph&, uint64_t&, argc, argv, MPI_Comm&, rank, nranks)
+ * (src/jupiter_gpm.cu:27), the loader Graph(prefix, use_dag) (include/graph.h:41-42) and
+ * the device set-operation templates (include/set_intersect.cuh, include/set_difference.cuh).
+ */
+#ifndef JGPM_H_
+#define JGPM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define JGPM_OK 0
+#define JGPM_EINVAL (-1)     /* bad argument or malformed graph */
+#define JGPM_ENOMEM (-2)     /* device or host allocation failed */
+#define JGPM_ECUDA (-3)      /* CUDA runtime error */
+#define JGPM_EIO (-4)        /* graph file missing or unreadable */
+#define JGPM_EPATTERN (-5)   /* unknown pattern name, or pattern/induced combination */
+#define JGPM_ETIMEDOUT (-6)  /* a bounded device wait gave up */
+#define JGPM_EOVERFLOW (-7)  /* a count does not fit in uint64 */
+#define JGPM_ENODEV (-8)     /* no CUDA device */
+#define JGPM_EBUSY (-9)      /* the server has no free slot */
+#define JGPM_ECAPACITY (-10) /* a per-root list exceeded a fixed capacity */
+#define JGPM_EADMISSION (-11)/* a query or graph does not fit the memory budget */
+#define JGPM_ENOTFOUND (-12) /* unknown ticket or graph id */
+
+typedef struct jgpm_graph jgpm_graph;
+
+typedef struct {
+  int32_t num_vertices;
+  int64_t num_arcs;        /* symmetric CSR slots (2 x undirected edges) */
+  int32_t max_degree;
+  int64_t num_dag_arcs;    /* 0 until the degree-oriented DAG is built */
+  int32_t max_out_degree;
+  int32_t device;
+  uint64_t device_bytes;   /* device memory held by the handle */
+} jgpm_graph_info;
+
+typedef struct {
+  uint64_t count;          /* the pattern count (also written to *out) */
+  uint64_t setop_elements; /* algorithmic set-op elements of the canonical plan; filled only
+                              when JGPM_COUNT_STATS is set */
+  double kernel_ms;        /* device time of the counting launches (CUDA events) */
+  int32_t rounds;          /* root-range rounds launched */
+  int32_t method;          /* implementation path taken (JGPM_METHOD_*) */
+  int32_t launches;        /* kernels launched by the counting call (timed part) */
+  int32_t reserved;
+} jgpm_stats;
+
+#define JGPM_METHOD_BITMAP_CLIQUE 1  /* vertex-rooted local-bitmap k-clique kernels */
+#define JGPM_METHOD_PLAN 2           /* per-root nested-loop plan kernel */
+#define JGPM_METHOD_WEDGE 3          /* wedge aggregation (4-cycle) */
+#define JGPM_METHOD_EDGE_TRIANGLE 4  /* per-edge triangle counts (diamond, census) */
+#define JGPM_METHOD_CENSUS 5         /* vertex-induced counts from the 4-vertex census */
+
+#define JGPM_COUNT_STATS 1u          /* also compute setop_elements (an extra untimed pass) */
+#define JGPM_COUNT_FORCE_PLAN 2u     /* use the literal nested-loop plan kernel */
+#define JGPM_COUNT_FORCE_ENUM 4u     /* vertex-induced patterns: enumerate with set difference */
+
+/* ---- library --------------------------------------------------------------------- */
+const char* jgpm_version(void);
+/* Message of the calling thread's last failed call ("" if none). */
+const char* jgpm_last_error(void);
+/* Number of visible CUDA devices. */
+int jgpm_device_count(int* n);
+/* Selects the device used by graphs created afterwards on this thread. */
+int jgpm_set_device(int device);
+
+/* ---- graphs ---------------------------------------------------------------------- */
+/* Loads prefix.meta.txt / prefix.vertex.bin (int64 row pointers) / prefix.edge.bin (int32
+ * sorted neighbour lists), the reference's on-disk CSR.  Replaces Graph::Graph(prefix,
+ * use_dag) (common/graph.cc:8-124, include/graph.h:41-42).  orient_dag=1 builds the
+ * degree-oriented DAG eagerly (Graph::orientation, common/graph.cc:210-401); the symmetric
+ * CSR is kept either way, and every pattern picks the CSR its plan needs. */
+int jgpm_graph_load(const char* prefix, int orient_dag, jgpm_graph** g);
+
+/* Builds a graph from a host symmetric CSR (sorted, duplicate-free rows, no self-loops, both
+ * directions present).  Replaces the CSR half of the reference loader and
+ * NvsGraphGPU::init (include/graph_gpu_nvs.h:243-304).  Malformed input gives JGPM_EINVAL. */
+int jgpm_graph_from_csr(const int64_t* rowptr, const int32_t* col, int32_t n, int64_t m,
+                        int orient_dag, jgpm_graph** g);
+
+/* Builds a graph from an undirected host edge list: both directions are added, self-loops
+ * dropped, rows sorted and deduplicated on the device.  (The reference reads prebuilt CSRs
+ * only; this is the ingest step before its loader.) */
+int jgpm_graph_from_edges(const int32_t* src, const int32_t* dst, int64_t num_edges,
+                          int32_t n, int orient_dag, jgpm_graph** g);
+
+/* Generates a seeded R-MAT graph on the device: edge i draws its quadrants from a
+ * counter-based hash of (seed, i) with integer thresholds, so the result does not depend on
+ * the thread layout; ids >= n are redrawn.  Then symmetrised, deduplicated, self-loops
+ * dropped.  No reference counterpart (the reference reads external datasets). */
+int jgpm_graph_rmat(int64_t n, int64_t num_edges, double a, double b, double c, uint64_t seed,
+                    int orient_dag, jgpm_graph** g);
+
+/* The same seeded R-MAT edges on the host (no GPU needed): writes up to num_edges pairs and
+ * the number written (edges with no valid draw in 64 attempts are dropped). */
+int jgpm_rmat_edges(int64_t n, int64_t num_edges, double a, double b, double c, uint64_t seed,
+                    int32_t* src, int32_t* dst, int64_t* out_count);
+
+int jgpm_graph_get_info(const jgpm_graph* g, jgpm_graph_info* info);
+
+/* Copies the symmetric CSR (dag=0) or the DAG (dag=1, built if needed) to host arrays of
+ * n+1 and num_arcs / num_dag_arcs entries. */
+int jgpm_graph_copy_csr(jgpm_graph* g, int dag, int64_t* rowptr, int32_t* col);
+
+/* Writes the symmetric CSR (dag=0) or the DAG (dag=1) in the reference's on-disk format.
+ * Replaces Graph::dump_binary (common/graph.cc:727-753). */
+int jgpm_graph_save(jgpm_graph* g, const char* prefix, int dag);
+
+void jgpm_graph_free(jgpm_graph* g);
+
+/* The CUDA stream (a cudaStream_t, as an opaque pointer) on which every kernel of this graph
+ * runs, so callers can order their own work or record events on it.  No reference
+ * counterpart. */
+int jgpm_graph_stream(jgpm_graph* g, void** stream);
+
+/* ---- counting -------------------------------------------------------------------- */
+/* Counts `pattern` in g exactly.  Replaces SubgraphSolver's pattern dispatch, round loop and
+ * count reduction (src/jupiter_gpm.cu:356-375, 393-428, 873-908).  Pattern names:
+ *   reference IDs  "P1".."P16", "vsgm_last_pattern" (edge-induced, reference semantics);
+ *   aliases        "triangle" (= P0 on the DAG), "4-clique" (= P13), "5-clique" (= P14),
+ *                  "6-clique", "7-clique", "k-clique:<k>" (3 <= k <= 8), "4-cycle" (= P1),
+ *                  "diamond" (= P2), "tailed-triangle", "4-path", "3-star".
+ * induced=0 counts edge-induced copies (reference semantics); induced=1 counts
+ * vertex-induced copies of the 4-vertex patterns (each 4-vertex subset whose induced
+ * subgraph is isomorphic to the pattern, once).  chunk_size is the reference's round count
+ * (the root range is split into that many launches; <= 1 means one); it does not change
+ * the result.  st may be NULL. */
+int jgpm_count(jgpm_graph* g, const char* pattern, int induced, int chunk_size, uint64_t* out,
+               jgpm_stats* st);
+
+/* jgpm_count with JGPM_COUNT_* flags. */
+int jgpm_count_ex(jgpm_graph* g, const char* pattern, int induced, int chunk_size,
+                  unsigned flags, uint64_t* out, jgpm_stats* st);
+
+/* Vertex-induced census of the six connected 4-vertex graphlets, out[0..5] = 3-star,
+ * 4-path, tailed triangle, 4-cycle, diamond, 4-clique. */
+int jgpm_census4(jgpm_graph* g, uint64_t out[6], jgpm_stats* st);
+
+/* ---- set operations -------------------------------------------------------------- */
+#define JGPM_OP_INTERSECT 0        /* materialise {x in A & B : x < upper} */
+#define JGPM_OP_INTERSECT_COUNT 1  /* |{x in A & B : x < upper, x != exclude}| */
+#define JGPM_OP_DIFFERENCE 2       /* materialise {x in A \ B : x < upper, x != exclude} */
+#define JGPM_OP_DIFFERENCE_COUNT 3 /* |{x in A \ B : x < upper, x != exclude}| */
+
+/* One sorted-set operation on int32 lists (device or host pointers; host buffers are
+ * staged).  upper = INT32_MAX for no bound; exclude = -1 for none.  For the materialising
+ * ops `out` must hold min(na, nb) (intersect) or na (difference) entries.  Replaces the
+ * warp templates intersect / intersect_num (include/set_intersect.cuh:107-115, 190-195,
+ * 352-360, 430-472) and difference_set / difference_num (include/set_difference.cuh:41-48,
+ * 96-102, 163-170, 239-245) and the VertexSet operators (include/VertexSet.h:53-160).
+ * Note: the reference's difference_num returns 0 when B is empty
+ * (include/set_difference.cuh:44-45); this entry point returns |A'| as the set algebra
+ * says. */
+int jgpm_setop(int op, const int32_t* a, int32_t na, const int32_t* b, int32_t nb,
+               int32_t upper, int32_t exclude, int32_t* out, int32_t* out_n);
+
+/* A batch of set operations in one launch: pair i is A = a[a_off[i] .. a_off[i+1]) and
+ * B = b[b_off[i] .. b_off[i+1]), with per-pair bounds (upper/exclude arrays may be NULL).
+ * Counts go to counts[i]; for the materialising ops results go to out[out_off[i] ..) where
+ * out_off (nops+1 entries, host) gives each pair's capacity.  Host or device arrays. */
+int jgpm_setop_batch(int op, const int32_t* a, const int64_t* a_off, const int32_t* b,
+                     const int64_t* b_off, int64_t nops, const int32_t* upper,
+                     const int32_t* exclude, int32_t* counts, int32_t* out,
+                     const int64_t* out_off);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JGPM_H_ */

@@ -1,0 +1,311 @@
+"""jupiter_b200 -- B200-native subgraph-pattern counting behind a plain C-ABI.
+
+The compute lives in ``libjgpm.so`` (hand-written CUDA for sm_100a, built in-tree by
+``jupiter_b200.build``); this module is a thin ctypes host layer that mirrors the
+reference's operator surface:
+
+* ``Graph.load(prefix, use_dag)``   -- Graph::Graph(prefix, use_dag) (include/graph.h:41-42)
+* ``Graph.count(pattern, ...)``     -- SubgraphSolver's pattern dispatch, round loop and
+                                       count reduction (src/jupiter_gpm.cu:356-908)
+* ``setop(...)`` / ``setop_batch``  -- the intersect / difference templates
+                                       (include/set_intersect.cuh, include/set_difference.cuh)
+* ``solve(prefix, pattern, rounds)`` -- the CLI `jupiter_gpm <graph> <pattern> [rounds]`
+                                       (src/main.cc:7-47), printing the same result line.
+
+There is no CPU fallback: importing works without a GPU (so the library can be inspected),
+but every compute call raises ``JgpmError`` when the library or a CUDA device is missing.
+"""
+import ctypes
+import os
+import time
+
+import numpy as np
+
+__all__ = [
+    "JgpmError", "Graph", "setop", "setop_batch", "solve", "lib", "library_path",
+    "OP_INTERSECT", "OP_INTERSECT_COUNT", "OP_DIFFERENCE", "OP_DIFFERENCE_COUNT",
+    "COUNT_STATS", "COUNT_FORCE_PLAN", "COUNT_FORCE_ENUM", "STATUS",
+]
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+
+OP_INTERSECT, OP_INTERSECT_COUNT, OP_DIFFERENCE, OP_DIFFERENCE_COUNT = 0, 1, 2, 3
+COUNT_STATS, COUNT_FORCE_PLAN, COUNT_FORCE_ENUM = 1, 2, 4
+
+STATUS = {
+    0: "JGPM_OK", -1: "JGPM_EINVAL", -2: "JGPM_ENOMEM", -3: "JGPM_ECUDA", -4: "JGPM_EIO",
+    -5: "JGPM_EPATTERN", -6: "JGPM_ETIMEDOUT", -7: "JGPM_EOVERFLOW", -8: "JGPM_ENODEV",
+    -9: "JGPM_EBUSY", -10: "JGPM_ECAPACITY", -11: "JGPM_EADMISSION", -12: "JGPM_ENOTFOUND",
+}
+METHODS = {1: "bitmap-clique", 2: "plan", 3: "wedge", 4: "edge-triangle", 5: "census"}
+
+_P64 = ctypes.POINTER(ctypes.c_int64)
+_P32 = ctypes.POINTER(ctypes.c_int32)
+_PU64 = ctypes.POINTER(ctypes.c_uint64)
+
+
+class JgpmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _GraphInfo(ctypes.Structure):
+    _fields_ = [("num_vertices", ctypes.c_int32), ("num_arcs", ctypes.c_int64),
+                ("max_degree", ctypes.c_int32), ("num_dag_arcs", ctypes.c_int64),
+                ("max_out_degree", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("device_bytes", ctypes.c_uint64)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint64), ("setop_elements", ctypes.c_uint64),
+                ("kernel_ms", ctypes.c_double), ("rounds", ctypes.c_int32),
+                ("method", ctypes.c_int32), ("launches", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+def library_path():
+    return os.environ.get("JGPM_LIBRARY", os.path.join(_PKG, "libjgpm.so"))
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libjgpm.so (raises JgpmError if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise JgpmError(-8, f"{path} is missing; run `python -m jupiter_b200.build`")
+    L = ctypes.CDLL(path)
+    L.jgpm_version.restype = ctypes.c_char_p
+    L.jgpm_last_error.restype = ctypes.c_char_p
+    L.jgpm_device_count.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    L.jgpm_set_device.argtypes = [ctypes.c_int]
+    G = ctypes.c_void_p
+    PG = ctypes.POINTER(ctypes.c_void_p)
+    L.jgpm_graph_load.argtypes = [ctypes.c_char_p, ctypes.c_int, PG]
+    L.jgpm_graph_from_csr.argtypes = [_P64, _P32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int,
+                                      PG]
+    L.jgpm_graph_from_edges.argtypes = [_P32, _P32, ctypes.c_int64, ctypes.c_int32,
+                                        ctypes.c_int, PG]
+    L.jgpm_graph_rmat.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
+                                  ctypes.c_int, PG]
+    L.jgpm_rmat_edges.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_uint64, _P32, _P32,
+                                  _P64]
+    L.jgpm_graph_get_info.argtypes = [G, ctypes.POINTER(_GraphInfo)]
+    L.jgpm_graph_copy_csr.argtypes = [G, ctypes.c_int, _P64, _P32]
+    L.jgpm_graph_save.argtypes = [G, ctypes.c_char_p, ctypes.c_int]
+    L.jgpm_graph_free.argtypes = [G]
+    L.jgpm_graph_free.restype = None
+    L.jgpm_graph_stream.argtypes = [G, ctypes.POINTER(ctypes.c_void_p)]
+    L.jgpm_count.argtypes = [G, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _PU64,
+                             ctypes.POINTER(_Stats)]
+    L.jgpm_count_ex.argtypes = [G, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_uint,
+                                _PU64, ctypes.POINTER(_Stats)]
+    L.jgpm_census4.argtypes = [G, _PU64, ctypes.POINTER(_Stats)]
+    L.jgpm_setop.argtypes = [ctypes.c_int, _P32, ctypes.c_int32, _P32, ctypes.c_int32,
+                             ctypes.c_int32, ctypes.c_int32, _P32, _P32]
+    L.jgpm_setop_batch.argtypes = [ctypes.c_int, _P32, _P64, _P32, _P64, ctypes.c_int64, _P32,
+                                   _P32, _P32, _P32, _P64]
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise JgpmError(rc, lib().jgpm_last_error().decode())
+
+
+def _p32(a):
+    return a.ctypes.data_as(_P32)
+
+
+def _p64(a):
+    return a.ctypes.data_as(_P64)
+
+
+def device_count():
+    n = ctypes.c_int()
+    _check(lib().jgpm_device_count(ctypes.byref(n)))
+    return n.value
+
+
+def version():
+    return lib().jgpm_version().decode()
+
+
+def rmat_edges(n, num_edges, a=0.57, b=0.19, c=0.19, seed=1):
+    """The seeded R-MAT edge list computed on the host (the device generator's definition)."""
+    src = np.empty(max(num_edges, 1), dtype=np.int32)
+    dst = np.empty(max(num_edges, 1), dtype=np.int32)
+    k = ctypes.c_int64()
+    _check(lib().jgpm_rmat_edges(int(n), int(num_edges), a, b, c, int(seed), _p32(src),
+                                 _p32(dst), ctypes.byref(k)))
+    return src[: k.value].copy(), dst[: k.value].copy()
+
+
+class Graph:
+    """A graph resident on one GPU (symmetric CSR, plus the degree-oriented DAG on demand)."""
+
+    def __init__(self, handle):
+        self._h = ctypes.c_void_p(handle)
+
+    # -- constructors ---------------------------------------------------------------
+    @classmethod
+    def load(cls, prefix, use_dag=False):
+        """Reads the reference's prefix.meta.txt/.vertex.bin/.edge.bin CSR."""
+        h = ctypes.c_void_p()
+        _check(lib().jgpm_graph_load(prefix.encode(), int(bool(use_dag)), ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_csr(cls, rowptr, col, use_dag=False):
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        h = ctypes.c_void_p()
+        _check(lib().jgpm_graph_from_csr(_p64(rowptr), _p32(col), len(rowptr) - 1, len(col),
+                                         int(bool(use_dag)), ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_edges(cls, src, dst, n, use_dag=False):
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        dst = np.ascontiguousarray(dst, dtype=np.int32)
+        h = ctypes.c_void_p()
+        _check(lib().jgpm_graph_from_edges(_p32(src), _p32(dst), len(src), int(n),
+                                           int(bool(use_dag)), ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def rmat(cls, n, edge_factor, a=0.57, b=0.19, c=0.19, seed=1, use_dag=False):
+        """Seeded R-MAT graph generated on the device (edge_factor * n edges drawn)."""
+        h = ctypes.c_void_p()
+        _check(lib().jgpm_graph_rmat(int(n), int(edge_factor) * int(n), a, b, c, int(seed),
+                                     int(bool(use_dag)), ctypes.byref(h)))
+        return cls(h.value)
+
+    # -- queries ----------------------------------------------------------------------
+    def info(self):
+        i = _GraphInfo()
+        _check(lib().jgpm_graph_get_info(self._h, ctypes.byref(i)))
+        return {f: getattr(i, f) for f, _ in _GraphInfo._fields_}
+
+    def csr(self, dag=False):
+        if dag:
+            self.count("triangle")  # builds the DAG if needed
+        info = self.info()
+        m = info["num_dag_arcs"] if dag else info["num_arcs"]
+        rowptr = np.empty(info["num_vertices"] + 1, dtype=np.int64)
+        col = np.empty(max(m, 1), dtype=np.int32)
+        _check(lib().jgpm_graph_copy_csr(self._h, int(bool(dag)), _p64(rowptr), _p32(col)))
+        return rowptr, col[:m].copy()
+
+    def stream(self):
+        """The cudaStream_t (as an int) on which this graph's kernels run."""
+        s = ctypes.c_void_p()
+        _check(lib().jgpm_graph_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def save(self, prefix, dag=False):
+        _check(lib().jgpm_graph_save(self._h, prefix.encode(), int(bool(dag))))
+
+    def count(self, pattern, induced=False, chunk_size=1, stats=False, flags=0, details=False):
+        """Exact count of `pattern`.  With stats=True (the canonical plan's set-op elements,
+        an extra untimed pass) or details=True returns (count, dict)."""
+        out = ctypes.c_uint64()
+        st = _Stats()
+        f = flags | (COUNT_STATS if stats else 0)
+        _check(lib().jgpm_count_ex(self._h, pattern.encode(), int(bool(induced)),
+                                   int(chunk_size), f, ctypes.byref(out), ctypes.byref(st)))
+        if stats or details:
+            return out.value, {"count": st.count, "setop_elements": st.setop_elements,
+                               "kernel_ms": st.kernel_ms, "rounds": st.rounds,
+                               "method": METHODS.get(st.method, st.method),
+                               "launches": st.launches}
+        return out.value
+
+    def census4(self):
+        """Vertex-induced counts [3-star, 4-path, tailed triangle, 4-cycle, diamond, K4]."""
+        out = np.zeros(6, dtype=np.uint64)
+        st = _Stats()
+        _check(lib().jgpm_census4(self._h, out.ctypes.data_as(_PU64), ctypes.byref(st)))
+        return [int(x) for x in out]
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().jgpm_graph_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def setop(op, a, b, upper=None, exclude=None):
+    """One sorted-set operation; returns a count (the *_COUNT ops) or an int32 array."""
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    b = np.ascontiguousarray(b, dtype=np.int32)
+    up = np.iinfo(np.int32).max if upper is None else int(upper)
+    ex = -1 if exclude is None else int(exclude)
+    cap = min(len(a), len(b)) if op == OP_INTERSECT else len(a)
+    out = np.empty(max(cap, 1), dtype=np.int32)
+    n = ctypes.c_int32()
+    _check(lib().jgpm_setop(op, _p32(a), len(a), _p32(b), len(b), up, ex, _p32(out),
+                            ctypes.byref(n)))
+    if op in (OP_INTERSECT_COUNT, OP_DIFFERENCE_COUNT):
+        return n.value
+    return out[: n.value].copy()
+
+
+def setop_batch(op, a_lists, b_lists, upper=None, exclude=None):
+    """Many set operations in one launch; returns counts (and result lists when materialising)."""
+    a_off = np.zeros(len(a_lists) + 1, dtype=np.int64)
+    b_off = np.zeros(len(b_lists) + 1, dtype=np.int64)
+    a_off[1:] = np.cumsum([len(x) for x in a_lists])
+    b_off[1:] = np.cumsum([len(x) for x in b_lists])
+    a = np.concatenate([np.asarray(x, dtype=np.int32) for x in a_lists] + [np.zeros(0, np.int32)])
+    b = np.concatenate([np.asarray(x, dtype=np.int32) for x in b_lists] + [np.zeros(0, np.int32)])
+    nops = len(a_lists)
+    counts = np.zeros(max(nops, 1), dtype=np.int32)
+    up = None if upper is None else np.ascontiguousarray(upper, dtype=np.int32)
+    ex = None if exclude is None else np.ascontiguousarray(exclude, dtype=np.int32)
+    mat = op in (OP_INTERSECT, OP_DIFFERENCE)
+    out = out_off = None
+    if mat:
+        caps = [min(len(x), len(y)) if op == OP_INTERSECT else len(x)
+                for x, y in zip(a_lists, b_lists)]
+        out_off = np.zeros(nops + 1, dtype=np.int64)
+        out_off[1:] = np.cumsum(caps)
+        out = np.empty(max(int(out_off[-1]), 1), dtype=np.int32)
+    _check(lib().jgpm_setop_batch(op, _p32(a), _p64(a_off), _p32(b), _p64(b_off), nops,
+                                  _p32(up) if up is not None else None,
+                                  _p32(ex) if ex is not None else None, _p32(counts),
+                                  _p32(out) if mat else None, _p64(out_off) if mat else None))
+    counts = counts[:nops]
+    if mat:
+        return counts, [out[out_off[i]: out_off[i] + counts[i]].copy() for i in range(nops)]
+    return counts
+
+
+def solve(prefix, pattern, rounds=1, print_result=True):
+    """The reference CLI flow (src/main.cc:7-47, src/jupiter_gpm.cu:27-925) on one GPU:
+    load, orient for the clique patterns, count, print `gpu count:<n>  runtime:<s>s`."""
+    use_dag = pattern in ("P13", "P14", "P15", "P16")
+    with Graph.load(prefix, use_dag=use_dag) as g:
+        c, st = g.count(pattern, chunk_size=rounds, details=True)
+    if print_result:
+        print(f"=====================gpu count:{c}  runtime:{st['kernel_ms'] / 1e3:.6f}s")
+    return c

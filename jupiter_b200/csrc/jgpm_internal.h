@@ -1,0 +1,112 @@
+// Internal declarations shared by the CUDA translation units of libjgpm.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/jgpm.h"
+
+namespace jgpm {
+
+typedef int32_t vid_t;
+typedef int64_t eid_t;
+typedef unsigned long long acc_t;
+
+// Device view of a CSR: row pointers (n+1, int64) and sorted neighbour lists (int32).
+struct DevCsr {
+  vid_t n;
+  eid_t m;
+  const eid_t* rowptr;
+  const vid_t* col;
+};
+
+// Roots of a clique count (vertices with DAG out-degree >= min_deg), sorted by out-degree
+// descending, so the array holds three tiers back to back:
+//   large  [0, large_end)          d > kMidMaxDeg
+//   mid    [large_end, mid_end)    32 < d <= kMidMaxDeg
+//   small  [mid_end, small_end)    min_deg <= d <= 32
+constexpr int kMidMaxDeg = 1024;
+
+struct RootTiers {
+  vid_t* d_roots = nullptr;
+  int64_t large_end = 0, mid_end = 0, small_end = 0;
+  int min_deg = -1;  // smallest out-degree kept
+};
+
+struct jgpm_graph_impl;
+
+// Per-launch device control block: work counters, results and the error word.
+struct DevControl {
+  unsigned long long counter[8];  // work-stealing cursors
+  unsigned long long count[4];    // pattern results
+  unsigned long long elements[4]; // set-op elements (stats launches)
+  int error;                      // JGPM_E* raised inside a kernel (0 = none)
+  int error_info;
+  int pad[14];
+};
+
+std::string cuda_error_string(cudaError_t e);
+
+}  // namespace jgpm
+
+// The opaque graph handle of the C-ABI.
+struct jgpm_graph {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int32_t n = 0;
+  // symmetric CSR
+  int64_t m = 0;
+  int64_t* d_rowptr = nullptr;
+  int32_t* d_col = nullptr;
+  int32_t max_degree = 0;
+  // degree-oriented DAG (built on demand)
+  int64_t m_dag = 0;
+  int64_t* d_dag_rowptr = nullptr;
+  int32_t* d_dag_col = nullptr;
+  int32_t max_out_degree = 0;
+  jgpm::RootTiers tiers;
+  // per-graph reusable launch state
+  jgpm::DevControl* d_ctl = nullptr;
+  jgpm::DevControl* h_ctl = nullptr;  // pinned mirror
+  void* d_scratch = nullptr;          // per-CTA scratch for heavy roots
+  size_t scratch_bytes = 0;
+  // statistics of the last count
+  double last_kernel_ms = 0.0;
+  int launches = 0;  // kernels launched since the counting call began
+  std::string name;
+};
+
+#define JGPM_CUDA_TRY(expr)                                   \
+  do {                                                        \
+    cudaError_t _e = (expr);                                  \
+    if (_e != cudaSuccess) {                                  \
+      jgpm_set_error_(std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+      return (_e == cudaErrorMemoryAllocation) ? JGPM_ENOMEM : JGPM_ECUDA; \
+    }                                                         \
+  } while (0)
+
+void jgpm_set_error_(const std::string& msg);
+
+namespace jgpm {
+// graph_build.cu
+int build_from_edges_device(jgpm_graph* g, int32_t n, int64_t* d_keys, int64_t nkeys_valid_cap);
+int rmat_build(jgpm_graph* g, int64_t n, int64_t num_edges, double a, double b, double c,
+               uint64_t seed);
+int upload_csr(jgpm_graph* g, const int64_t* rowptr, const int32_t* col, int32_t n, int64_t m,
+               int validate);
+int ensure_dag(jgpm_graph* g);
+int ensure_tiers(jgpm_graph* g, int min_deg);
+int ensure_control(jgpm_graph* g);
+int ensure_scratch(jgpm_graph* g, size_t bytes);
+void free_graph_device(jgpm_graph* g);
+int device_sm_count(int device);
+// k-clique count through the bitmap kernels (capi.cu)
+int count_clique_public(jgpm_graph* g, int k, uint64_t* out, double* ms);
+// non-clique dispatch (plans.cu); *method receives a JGPM_METHOD_* code
+int count_plan_impl(jgpm_graph* g, int id, int chunk_size, unsigned flags, bool stats,
+                    uint64_t* out, uint64_t* elements, double* ms, int* method);
+int plan_id_of(const std::string& name, int induced);
+bool plan_uses_dag(int plan_id);
+int count_census4(jgpm_graph* g, uint64_t out[6], double* ms);
+}  // namespace jgpm
