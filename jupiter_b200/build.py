@@ -63,7 +63,24 @@ def build(force=False, verbose=False, extra=None):
         if r.returncode != 0:
             sys.stderr.write(r.stdout)
             raise RuntimeError("link of libjgpm.so failed")
+    build_cli(force=force or bool(jobs))
     return LIB
+
+
+def build_cli(force=False):
+    """The jupiter_gpm command-line front end (host C++ over the C-ABI), rpath'd to the lib."""
+    src = os.path.join(PKG, "cli", "jupiter_gpm.cc")
+    out = os.path.join(PKG, "jupiter_gpm")
+    if not force and os.path.exists(out) and os.path.getmtime(out) > max(
+            os.path.getmtime(src), os.path.getmtime(LIB)):
+        return out
+    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), src, "-o", out,
+           "-L", PKG, "-ljgpm", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout)
+        raise RuntimeError("build of jupiter_gpm failed")
+    return out
 
 
 if __name__ == "__main__":

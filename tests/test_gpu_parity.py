@@ -186,7 +186,8 @@ def test_malformed_csr_rejected(gpu):
         (ok_rowptr, np.array([2, 1, 0, 2, 0, 1], dtype=np.int32)),      # unsorted row
         (ok_rowptr, np.array([1, 2, 0, 2, 0, 3], dtype=np.int32)),      # id out of range
         (ok_rowptr, np.array([0, 2, 0, 2, 0, 1], dtype=np.int32)),      # self-loop
-        (np.array([0, 2, 3, 4], dtype=np.int64), np.array([1, 2, 0, 0], dtype=np.int32)),
+        (np.array([0, 2, 3, 4], dtype=np.int64), np.array([1, 2, 0, 1], dtype=np.int32)),
+        # ^ asymmetric: 2 lists 1, but 1 does not list 2
         (np.array([0, 3, 2, 6], dtype=np.int64), ok_col),               # decreasing rowptr
         (np.array([0, 2, 4, 5], dtype=np.int64), ok_col),               # rowptr[n] != m
         (ok_rowptr, np.array([1, 2, 0, 2, 1, 1], dtype=np.int32)),      # duplicate / asymmetric
