@@ -153,6 +153,47 @@ int jgpm_count_ex(jgpm_graph* g, const char* pattern, int induced, int chunk_siz
  * 4-path, tailed triangle, 4-cycle, diamond, 4-clique. */
 int jgpm_census4(jgpm_graph* g, uint64_t out[6], jgpm_stats* st);
 
+/* ---- batched counting -------------------------------------------------------------- */
+/* One (graph, pattern) job.  Batchable patterns: "triangle", "4-clique" .. "7-clique",
+ * "k-clique:<k>", "diamond" (= P2) and "4-cycle" (= P1), all with reference semantics. */
+typedef struct {
+  jgpm_graph* graph;
+  const char* pattern;
+} jgpm_job;
+
+/* Work-split knobs of the batched kernel (and of the plain clique kernels). */
+typedef struct {
+  int32_t min_group;      /* narrowest lane group for roots of out-degree <= 32: 4, 8, 16, 32 */
+  int32_t split_degree;   /* roots with out-degree above this (<= 32) run CTA-wide */
+  int32_t roots_per_task; /* roots per queued task (edges per task = 8x, apexes = 1/4x) */
+  int32_t intersect;      /* edge set ops: 0 by length ratio (merge path or search), 1 search */
+} jgpm_tuning;
+
+typedef struct {
+  double kernel_ms;       /* device time of the batch (task upload + kernel + count read-back) */
+  int32_t launches;       /* kernels launched (1: one persistent launch for the whole batch) */
+  int32_t tasks;          /* tasks in the global queue */
+  jgpm_tuning used;
+} jgpm_batch_stats;
+
+/* Counts every job exactly in ONE persistent work-stealing launch: all jobs' work is cut into
+ * tasks of one global queue that persistent CTAs drain; counts[i] receives job i's count.
+ * Replaces, for a whole batch, the reference's per-query round loop and static chunking
+ * (src/jupiter_gpm.cu:356-375).  tuning = NULL uses the defaults.  All graphs must be on one
+ * device. */
+int jgpm_batch_count(const jgpm_job* jobs, int32_t njobs, const jgpm_tuning* tuning,
+                     uint64_t* counts, jgpm_batch_stats* st);
+
+/* Sets the lane-group and split knobs (min_group, split_degree) the plain clique kernels of
+ * this graph use; split_degree in {32, 64, 128} (roots of out-degree 32 < d <= split run one per
+ * warp, larger ones one per CTA).  Counts do not depend on it. */
+int jgpm_graph_set_tuning(jgpm_graph* g, const jgpm_tuning* tuning);
+
+/* Picks the tuning by timing candidate settings (coordinate descent over the four knobs) on
+ * an evenly spaced sample of at most sample_jobs jobs (<= 0: 256).  No reference
+ * counterpart. */
+int jgpm_autotune(const jgpm_job* jobs, int32_t njobs, int32_t sample_jobs, jgpm_tuning* out);
+
 /* ---- set operations -------------------------------------------------------------- */
 #define JGPM_OP_INTERSECT 0        /* materialise {x in A & B : x < upper} */
 #define JGPM_OP_INTERSECT_COUNT 1  /* |{x in A & B : x < upper, x != exclude}| */

@@ -24,7 +24,8 @@ import numpy as np
 __all__ = [
     "JgpmError", "Graph", "setop", "setop_batch", "solve", "lib", "library_path",
     "OP_INTERSECT", "OP_INTERSECT_COUNT", "OP_DIFFERENCE", "OP_DIFFERENCE_COUNT",
-    "COUNT_STATS", "COUNT_FORCE_PLAN", "COUNT_FORCE_ENUM", "STATUS",
+    "COUNT_STATS", "COUNT_FORCE_PLAN", "COUNT_FORCE_ENUM", "STATUS", "batch_count",
+    "autotune", "Tuning",
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -62,6 +63,24 @@ class _Stats(ctypes.Structure):
                 ("kernel_ms", ctypes.c_double), ("rounds", ctypes.c_int32),
                 ("method", ctypes.c_int32), ("launches", ctypes.c_int32),
                 ("reserved", ctypes.c_int32)]
+
+
+class _Job(ctypes.Structure):
+    _fields_ = [("graph", ctypes.c_void_p), ("pattern", ctypes.c_char_p)]
+
+
+class Tuning(ctypes.Structure):
+    """Work-split knobs of the batched (and plain clique) kernels."""
+    _fields_ = [("min_group", ctypes.c_int32), ("split_degree", ctypes.c_int32),
+                ("roots_per_task", ctypes.c_int32), ("intersect", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class _BatchStats(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("launches", ctypes.c_int32),
+                ("tasks", ctypes.c_int32), ("used", Tuning)]
 
 
 def library_path():
@@ -112,6 +131,11 @@ def lib():
                              ctypes.c_int32, ctypes.c_int32, _P32, _P32]
     L.jgpm_setop_batch.argtypes = [ctypes.c_int, _P32, _P64, _P32, _P64, ctypes.c_int64, _P32,
                                    _P32, _P32, _P32, _P64]
+    L.jgpm_batch_count.argtypes = [ctypes.POINTER(_Job), ctypes.c_int32, ctypes.POINTER(Tuning),
+                                   _PU64, ctypes.POINTER(_BatchStats)]
+    L.jgpm_graph_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
+    L.jgpm_autotune.argtypes = [ctypes.POINTER(_Job), ctypes.c_int32, ctypes.c_int32,
+                                ctypes.POINTER(Tuning)]
     _lib = L
     return L
 
@@ -205,6 +229,10 @@ class Graph:
         _check(lib().jgpm_graph_copy_csr(self._h, int(bool(dag)), _p64(rowptr), _p32(col)))
         return rowptr, col[:m].copy()
 
+    def set_tuning(self, tuning):
+        """Lane-group / split knobs of this graph's plain clique kernels (counts unchanged)."""
+        _check(lib().jgpm_graph_set_tuning(self._h, ctypes.byref(tuning)))
+
     def stream(self):
         """The cudaStream_t (as an int) on which this graph's kernels run."""
         s = ctypes.c_void_p()
@@ -252,6 +280,38 @@ class Graph:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def _jobs_array(jobs):
+    arr = (_Job * len(jobs))()
+    keep = []
+    for i, (g, pattern) in enumerate(jobs):
+        b = pattern.encode()
+        keep.append(b)
+        arr[i].graph = g._h.value
+        arr[i].pattern = b
+    return arr, keep
+
+
+def batch_count(jobs, tuning=None):
+    """Counts many (graph, pattern) jobs in one persistent launch.
+    Returns (counts, stats dict)."""
+    arr, keep = _jobs_array(jobs)
+    counts = np.zeros(max(len(jobs), 1), dtype=np.uint64)
+    st = _BatchStats()
+    _check(lib().jgpm_batch_count(arr, len(jobs), ctypes.byref(tuning) if tuning else None,
+                                  counts.ctypes.data_as(_PU64), ctypes.byref(st)))
+    return [int(x) for x in counts[:len(jobs)]], {
+        "kernel_ms": st.kernel_ms, "launches": st.launches, "tasks": st.tasks,
+        "tuning": st.used.as_dict()}
+
+
+def autotune(jobs, sample_jobs=256):
+    """Times candidate tunings on a sample of the batch; returns the fastest Tuning."""
+    arr, keep = _jobs_array(jobs)
+    t = Tuning()
+    _check(lib().jgpm_autotune(arr, len(jobs), int(sample_jobs), ctypes.byref(t)))
+    return t
 
 
 def setop(op, a, b, upper=None, exclude=None):

@@ -119,7 +119,7 @@ int count_clique(jgpm_graph* g, int k, int chunk_size, bool stats, uint64_t* out
   JGPM_CUDA_TRY(cudaEventCreate(&e0));
   JGPM_CUDA_TRY(cudaEventCreate(&e1));
   if ((rc = reset_control(g, s))) return rc;
-  const int64_t nroots = g->tiers.small_end;
+  const int64_t nroots = g->tiers.deg_begin[k - 2];
   const int rounds = chunk_size > 1 ? chunk_size : 1;
   const int64_t per = (nroots + rounds - 1) / rounds;
   JGPM_CUDA_TRY(cudaEventRecord(e0, s));
@@ -371,6 +371,24 @@ int jgpm_count_ex(jgpm_graph* g, const char* pattern, int induced, int chunk_siz
     st->launches = g->launches;
     st->reserved = 0;
   }
+  return JGPM_OK;
+}
+
+int jgpm_graph_set_tuning(jgpm_graph* g, const jgpm_tuning* t) {
+  if (!g || !t) {
+    jgpm_set_error_("jgpm_graph_set_tuning: null argument");
+    return JGPM_EINVAL;
+  }
+  if (t->min_group != 4 && t->min_group != 8 && t->min_group != 16 && t->min_group != 32) {
+    jgpm_set_error_("jgpm_graph_set_tuning: min_group must be 4, 8, 16 or 32");
+    return JGPM_EINVAL;
+  }
+  if (t->split_degree != 32 && t->split_degree != 64 && t->split_degree != 128) {
+    jgpm_set_error_("jgpm_graph_set_tuning: split_degree must be 32, 64 or 128");
+    return JGPM_EINVAL;
+  }
+  g->tune_min_group = t->min_group;
+  g->tune_split = t->split_degree;
   return JGPM_OK;
 }
 

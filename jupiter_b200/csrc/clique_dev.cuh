@@ -1,0 +1,450 @@
+// Device building blocks of the vertex-rooted local-bitmap k-clique count, shared by the
+// plain per-query kernels (clique.cu) and the batched persistent kernel (batch.cu).
+//
+// For a root u with out-degree d, L = N+(u) (sorted) and the bitmap rows
+//     R_i bit j  <=>  L[j] in N+(L[i])
+// are the level-1 sets of the reference's edge-rooted plans (W of arc (u, L[i]));
+// K_k(u) = sum_i C_{k-3}(R_i) with C_0(m) = popc(m), C_t(m) = sum_{j in m} C_{t-1}(m & R_j).
+#pragma once
+#include "jgpm_internal.h"
+#include "setops.cuh"
+
+namespace jgpm {
+
+constexpr int kRangeCut = 32;  // restrict a row to [L0, Ld-1] when longer than this
+
+// ---------------------------------------------------------------- single-word rows
+template <int D, bool STATS>
+struct SmallCount {
+  // m: candidate set (bits over L), R: rows, deg: out-degrees of L (stats only)
+  __device__ __forceinline__ static acc_t run(uint32_t m, const uint32_t* R, const int* deg,
+                                              acc_t& elems) {
+    acc_t s = 0;
+    const int pm = __popc(m);
+    uint32_t it = m;
+    while (it) {
+      const int j = __ffs(it) - 1;
+      it &= it - 1;
+      if (STATS) elems += (acc_t)pm + (acc_t)deg[j];
+      s += SmallCount<D - 1, STATS>::run(m & R[j], R, deg, elems);
+    }
+    return s;
+  }
+};
+
+template <bool STATS>
+struct SmallCount<0, STATS> {
+  __device__ __forceinline__ static acc_t run(uint32_t m, const uint32_t*, const int*, acc_t&) {
+    return (acc_t)__popc(m);
+  }
+};
+
+// One root per group of G lanes (G in {4, 8, 16, 32}); every lane of the warp calls this
+// with its group's root u (or u < 0 for an idle group).  R and DG point at the group's G
+// shared words.  Returns this lane's partial count.  tri (edge-triangle mode) receives one
+// count per triangle arc.
+template <int G, int K, bool STATS, bool ETRI>
+__device__ __forceinline__ acc_t group_root(const eid_t* __restrict__ rowptr,
+                                            const vid_t* __restrict__ col, vid_t u,
+                                            uint32_t* R, int* DG, uint32_t* tri,
+                                            acc_t& elems) {
+  const int lane = threadIdx.x & 31;
+  const int gl = lane & (G - 1);
+  eid_t base = 0;
+  int d = 0;
+  if (u >= 0) {
+    base = rowptr[u];
+    d = (int)(rowptr[u + 1] - base);
+  }
+  const vid_t Lj = gl < d ? __ldg(col + base + gl) : INT32_MAX;
+  const vid_t lo_key = __shfl_sync(kFull, Lj, 0, G);
+  const vid_t hi_key = __shfl_sync(kFull, Lj, d > 0 ? d - 1 : 0, G);
+  eid_t s = 0;
+  int len = 0;
+  if (gl < d) {
+    s = rowptr[Lj];
+    len = (int)(rowptr[Lj + 1] - s);
+    if (STATS) DG[gl] = len;
+    if (len > kRangeCut) {
+      const int lb = lower_bound_g(col + s, len, lo_key);
+      const int ub = upper_bound_g(col + s, len, hi_key);
+      s += lb;
+      len = ub > lb ? ub - lb : 0;
+    }
+  }
+  R[gl] = 0u;
+  int off = len;  // inclusive scan of the row lengths within the group
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, off, o, G);
+    if (gl >= o) off += t;
+  }
+  const int T = __shfl_sync(kFull, off, G - 1, G);
+  const int Tmax = (G == 32) ? T : (int)__reduce_max_sync(kFull, (unsigned)T);
+  const int row_start = off - len;
+  __syncwarp();
+  for (int t0 = 0; t0 < Tmax; t0 += G) {
+    const int t = t0 + gl;
+    // row i = number of rows of the group ending at or before t
+    int i = 0;
+#pragma unroll
+    for (int step = G / 2; step > 0; step >>= 1) {
+      const int ov = __shfl_sync(kFull, off, i + step - 1, G);
+      if (ov <= t) i += step;
+    }
+    const eid_t si = __shfl_sync(kFull, s, i, G);
+    const int sti = __shfl_sync(kFull, row_start, i, G);
+    const vid_t x = t < T ? __ldg(col + si + (t - sti)) : INT32_MIN;
+    int p = 0;
+#pragma unroll
+    for (int step = G / 2; step > 0; step >>= 1) {
+      const vid_t lv = __shfl_sync(kFull, Lj, p + step - 1, G);
+      if (lv < x) p += step;
+    }
+    const vid_t lp = __shfl_sync(kFull, Lj, p, G);
+    if (t < T && lp == x) {
+      atomicOr(&R[i], 1u << p);
+      if (ETRI) {  // triangle (u, L[i], L[p]): one count on each of its three arcs
+        atomicAdd(tri + si + (t - sti), 1u);
+        atomicAdd(tri + base + i, 1u);
+        atomicAdd(tri + base + p, 1u);
+      }
+    }
+  }
+  __syncwarp();
+  acc_t cnt = 0;
+  if (gl < d) cnt = SmallCount<K - 3, STATS>::run(R[gl], R, DG, elems);
+  __syncwarp();
+  return cnt;
+}
+
+// ---------------------------------------------------------------- multi-word rows
+template <int D, bool STATS>
+struct DistCount {
+  // Mask distributed one word per lane (lane w holds word w, w < W).
+  __device__ __forceinline__ static acc_t run(uint32_t mw, const uint32_t* R, int W,
+                                              const int* deg, acc_t& elems) {
+    const int lane = threadIdx.x & 31;
+    acc_t s = 0;
+    int pm = 0;
+    if (STATS) pm = __reduce_add_sync(kFull, (unsigned)__popc(mw));
+    unsigned nz = __ballot_sync(kFull, mw != 0u);
+    while (nz) {
+      const int lw = __ffs(nz) - 1;
+      nz &= nz - 1;
+      uint32_t word = __shfl_sync(kFull, mw, lw);
+      while (word) {
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        const int j = lw * 32 + b;
+        if (STATS && lane == 0) elems += (acc_t)pm + (acc_t)deg[j];
+        const uint32_t nxt = lane < W ? (mw & R[(size_t)j * W + lane]) : 0u;
+        s += DistCount<D - 1, STATS>::run(nxt, R, W, deg, elems);
+      }
+    }
+    return s;
+  }
+};
+
+template <bool STATS>
+struct DistCount<0, STATS> {
+  __device__ __forceinline__ static acc_t run(uint32_t mw, const uint32_t*, int, const int*,
+                                              acc_t&) {
+    return (acc_t)__popc(mw);  // per-lane partial; summed at the end
+  }
+};
+
+// Row-parallel counting with the candidate mask in registers (WMAX words, W <= WMAX used):
+// one thread owns one first-level row and walks the deeper levels itself.  Each level has a
+// single recursive call site (code size stays linear in the depth); words are picked out of
+// the register array with an unrolled select so the masks never go to local memory.
+template <int WMAX>
+__device__ __forceinline__ uint32_t pick_word(const uint32_t (&m)[WMAX], int w) {
+  uint32_t r = 0u;
+#pragma unroll
+  for (int q = 0; q < WMAX; ++q) r = (q == w) ? m[q] : r;
+  return r;
+}
+
+template <int D, int WMAX, bool STATS>
+struct RowCount {
+  __device__ static acc_t run(const uint32_t (&m)[WMAX], const uint32_t* R, int W,
+                              const int* deg, acc_t& elems) {
+    acc_t s = 0;
+    int pm = 0;
+    if (STATS) {
+#pragma unroll
+      for (int w = 0; w < WMAX; ++w) pm += __popc(m[w]);
+    }
+    int w = 0;
+    uint32_t bits = m[0];
+    for (;;) {
+      while (bits == 0u) {
+        if (++w >= W) return s;
+        bits = pick_word<WMAX>(m, w);
+      }
+      const int j = w * 32 + __ffs(bits) - 1;
+      bits &= bits - 1;
+      if (STATS) elems += (acc_t)pm + (acc_t)deg[j];
+      uint32_t nxt[WMAX];
+      const uint32_t* Rj = R + (size_t)j * W;
+#pragma unroll
+      for (int q = 0; q < WMAX; ++q) nxt[q] = q < W ? (m[q] & Rj[q]) : 0u;
+      s += RowCount<D - 1, WMAX, STATS>::run(nxt, R, W, deg, elems);
+    }
+  }
+};
+
+template <int WMAX, bool STATS>
+struct RowCount<0, WMAX, STATS> {
+  __device__ __forceinline__ static acc_t run(const uint32_t (&m)[WMAX], const uint32_t*, int,
+                                              const int*, acc_t&) {
+    acc_t s = 0;
+#pragma unroll
+    for (int w = 0; w < WMAX; ++w) s += (acc_t)__popc(m[w]);
+    return s;
+  }
+};
+
+// ---------------------------------------------------------------- warp per root
+// One root of out-degree 32 < d <= kWarpMaxDeg per warp, with the warp's own slice of shared
+// memory (no CTA barriers).
+constexpr int kWarpMaxDeg = 128;
+constexpr int kWarpW = kWarpMaxDeg / 32;
+
+struct WarpSmem {
+  vid_t L[kWarpMaxDeg];
+  int off[kWarpMaxDeg + 1];
+  int deg[kWarpMaxDeg];
+  eid_t rs[kWarpMaxDeg];
+  uint32_t R[kWarpMaxDeg * kWarpW];
+};
+
+template <int K, bool STATS, bool ETRI>
+__device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
+                                           const vid_t* __restrict__ col, vid_t u, WarpSmem& ws,
+                                           uint32_t* tri, acc_t& elems) {
+  const int lane = threadIdx.x & 31;
+  const eid_t base = rowptr[u];
+  const int d = (int)(rowptr[u + 1] - base);
+  const int w_d = (d + 31) >> 5;
+  for (int j = lane; j < d; j += 32) ws.L[j] = __ldg(col + base + j);
+  for (int q = lane; q < d * w_d; q += 32) ws.R[q] = 0u;
+  __syncwarp();
+  const vid_t lo_key = ws.L[0], hi_key = ws.L[d - 1];
+  for (int i = lane; i < d; i += 32) {
+    const vid_t v = ws.L[i];
+    eid_t s = rowptr[v];
+    int len = (int)(rowptr[v + 1] - s);
+    ws.deg[i] = len;
+    if (len > kRangeCut) {
+      const int lb = lower_bound_g(col + s, len, lo_key);
+      const int ub = upper_bound_g(col + s, len, hi_key);
+      s += lb;
+      len = ub > lb ? ub - lb : 0;
+    }
+    ws.rs[i] = s;
+    ws.off[i] = len;
+  }
+  __syncwarp();
+  {  // exclusive scan: lane takes rows [4 lane, 4 lane + 4)
+    const int b0 = min(d, lane * kWarpW), b1 = min(d, b0 + kWarpW);
+    int local = 0;
+    for (int i = b0; i < b1; ++i) local += ws.off[i];
+    int incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    int run = incl - local;
+    __syncwarp();
+    for (int i = b0; i < b1; ++i) {
+      const int l = ws.off[i];
+      ws.off[i] = run;
+      run += l;
+    }
+    if (lane == 31) ws.off[d] = incl;
+    __syncwarp();
+  }
+  const int T = ws.off[d];
+  for (int t = lane; t < T; t += 32) {
+    int lo = 0, hi = d - 1;  // row i: last i with off[i] <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (ws.off[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const int i = lo;
+    const vid_t x = __ldg(col + ws.rs[i] + (t - ws.off[i]));
+    int p0 = 0, p1 = d;
+    while (p0 < p1) {
+      const int mid = (p0 + p1) >> 1;
+      if (ws.L[mid] < x) p0 = mid + 1;
+      else p1 = mid;
+    }
+    if (p0 < d && ws.L[p0] == x) {
+      atomicOr(&ws.R[i * w_d + (p0 >> 5)], 1u << (p0 & 31));
+      if (ETRI) {
+        atomicAdd(tri + ws.rs[i] + (t - ws.off[i]), 1u);
+        atomicAdd(tri + base + i, 1u);
+        atomicAdd(tri + base + p0, 1u);
+      }
+    }
+  }
+  __syncwarp();
+  acc_t cnt = 0;
+  for (int i = lane; i < d; i += 32) {
+    uint32_t m[kWarpW];
+#pragma unroll
+    for (int q = 0; q < kWarpW; ++q) m[q] = q < w_d ? ws.R[i * w_d + q] : 0u;
+    cnt += RowCount<K - 3, kWarpW, STATS>::run(m, ws.R, w_d, ws.deg, elems);
+  }
+  __syncwarp();
+  return cnt;
+}
+
+// Shared layout for one mid-tier root (dynamic shared memory):
+//   L[dmax] ids | off[dmax+1] exclusive row offsets | rs[dmax] row starts (int64) |
+//   deg[dmax] | R[dmax * W] rows | 8 warp sums
+struct MidLayout {
+  int dmax, W;
+  __host__ __device__ size_t bytes() const {
+    return (size_t)dmax * 4 + (size_t)(dmax + 1) * 4 + (size_t)dmax * 8 + (size_t)dmax * 4 +
+           (size_t)dmax * W * 4 + 64 + 64;
+  }
+};
+
+struct MidSmem {
+  vid_t* L;
+  int* off;
+  eid_t* rs;
+  int* deg;
+  uint32_t* R;
+  int* wsum;
+  __device__ __forceinline__ static MidSmem carve(unsigned char* smem, int dmax, int W) {
+    MidSmem m;
+    m.L = reinterpret_cast<vid_t*>(smem);
+    m.off = reinterpret_cast<int*>(m.L + dmax);
+    m.rs = reinterpret_cast<eid_t*>(
+        (reinterpret_cast<uintptr_t>(m.off + dmax + 1) + 7) & ~uintptr_t(7));
+    m.deg = reinterpret_cast<int*>(m.rs + dmax);
+    m.R = reinterpret_cast<uint32_t*>(m.deg + dmax);
+    m.wsum = reinterpret_cast<int*>(m.R + (size_t)dmax * W);
+    return m;
+  }
+};
+
+// Rows up to this many words (out-degree <= 512) are counted row-parallel from registers.
+constexpr int kCtaRowWords = 16;
+
+// One root of out-degree 32 < d <= dmax processed by the whole CTA (blockDim = 256).
+// Every thread calls it; returns this thread's partial count.
+template <int K, bool STATS, bool ETRI>
+__device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
+                                          const vid_t* __restrict__ col, vid_t u,
+                                          const MidSmem& sm, uint32_t* tri, acc_t& elems) {
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int nthreads = blockDim.x;
+  const int nwarps = nthreads >> 5;
+  vid_t* L = sm.L;
+  int* off = sm.off;
+  eid_t* rs = sm.rs;
+  int* deg = sm.deg;
+  uint32_t* R = sm.R;
+  const eid_t base = rowptr[u];
+  const int d = (int)(rowptr[u + 1] - base);
+  const int w_d = (d + 31) >> 5;
+  for (int j = tid; j < d; j += nthreads) L[j] = __ldg(col + base + j);
+  for (int q = tid; q < d * w_d; q += nthreads) R[q] = 0u;
+  __syncthreads();
+  const vid_t lo_key = L[0], hi_key = L[d - 1];
+  for (int i = tid; i < d; i += nthreads) {
+    const vid_t v = L[i];
+    eid_t s = rowptr[v];
+    int len = (int)(rowptr[v + 1] - s);
+    deg[i] = len;
+    if (len > kRangeCut) {
+      const int lb = lower_bound_g(col + s, len, lo_key);
+      const int ub = upper_bound_g(col + s, len, hi_key);
+      s += lb;
+      len = ub > lb ? ub - lb : 0;
+    }
+    rs[i] = s;
+    off[i] = len;
+  }
+  __syncthreads();
+  {  // exclusive scan of off[0..d): blocked per thread, then across warps
+    const int per = (d + nthreads - 1) / nthreads;
+    const int b0 = min(d, tid * per), b1 = min(d, b0 + per);
+    int local = 0;
+    for (int i = b0; i < b1; ++i) local += off[i];
+    int incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) sm.wsum[warp] = incl;
+    __syncthreads();
+    int wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += sm.wsum[w];
+    int run = wbase + incl - local;
+    __syncthreads();
+    for (int i = b0; i < b1; ++i) {
+      const int l = off[i];
+      off[i] = run;
+      run += l;
+    }
+    if (tid == nthreads - 1) off[d] = run;
+    __syncthreads();
+  }
+  const int T = off[d];
+  for (int t = tid; t < T; t += nthreads) {
+    int lo = 0, hi = d - 1;  // row i: last i with off[i] <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (off[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const int i = lo;
+    const vid_t x = __ldg(col + rs[i] + (t - off[i]));
+    int p0 = 0, p1 = d;
+    while (p0 < p1) {
+      const int mid = (p0 + p1) >> 1;
+      if (L[mid] < x) p0 = mid + 1;
+      else p1 = mid;
+    }
+    if (p0 < d && L[p0] == x) {
+      atomicOr(&R[(size_t)i * w_d + (p0 >> 5)], 1u << (p0 & 31));
+      if (ETRI) {
+        atomicAdd(tri + rs[i] + (t - off[i]), 1u);
+        atomicAdd(tri + base + i, 1u);
+        atomicAdd(tri + base + p0, 1u);
+      }
+    }
+  }
+  __syncthreads();
+  acc_t cnt = 0;
+  if (w_d <= kCtaRowWords) {
+    // row-parallel: each thread owns rows, masks in registers
+    for (int i = tid; i < d; i += nthreads) {
+      uint32_t m[kCtaRowWords];
+#pragma unroll
+      for (int q = 0; q < kCtaRowWords; ++q) m[q] = q < w_d ? R[(size_t)i * w_d + q] : 0u;
+      cnt += RowCount<K - 3, kCtaRowWords, STATS>::run(m, R, w_d, deg, elems);
+    }
+  } else {
+    // very wide rows: the mask is distributed one word per lane
+    for (int i = warp; i < d; i += nwarps) {
+      const uint32_t mw = lane < w_d ? R[(size_t)i * w_d + lane] : 0u;
+      cnt += DistCount<K - 3, STATS>::run(mw, R, w_d, deg, elems);
+    }
+  }
+  __syncthreads();
+  return cnt;
+}
+
+}  // namespace jgpm

@@ -425,7 +425,10 @@ int ensure_dag(jgpm_graph* g) {
 int ensure_tiers(jgpm_graph* g, int min_deg) {
   int rc;
   if ((rc = ensure_dag(g))) return rc;
-  if (min_deg < 1) min_deg = 1;
+  // One root list serves every k: it keeps all roots with out-degree >= 2 and the kernels
+  // take the prefix with d >= k-1 (deg_begin).
+  (void)min_deg;
+  min_deg = 2;
   if (g->tiers.d_roots && g->tiers.min_deg == min_deg) return JGPM_OK;
   if (g->tiers.d_roots) {
     cudaFree(g->tiers.d_roots);
@@ -466,6 +469,26 @@ int ensure_tiers(jgpm_graph* g, int min_deg) {
   g->tiers.large_end = n_large;
   g->tiers.mid_end = n_large + n_mid;
   g->tiers.small_end = n_large + n_mid + n_small;
+  // deg_begin[x]: first index with out-degree <= x (keys are sorted descending)
+  for (int x = 0; x < 34; ++x) {
+    int64_t lo = 0, hi = g->tiers.small_end;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (hk[mid] > (uint32_t)x) lo = mid + 1;
+      else hi = mid;
+    }
+    g->tiers.deg_begin[x] = lo;
+  }
+  const uint32_t le_thr[3] = {32u, 64u, 128u};
+  for (int q = 0; q < 3; ++q) {
+    int64_t lo = 0, hi = g->tiers.small_end;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (hk[mid] > le_thr[q]) lo = mid + 1;
+      else hi = mid;
+    }
+    g->tiers.le_begin[q] = lo;
+  }
   g->tiers.min_deg = min_deg;
   return JGPM_OK;
 }

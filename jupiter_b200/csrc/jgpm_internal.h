@@ -28,9 +28,13 @@ struct DevCsr {
 //   small  [mid_end, small_end)    min_deg <= d <= 32
 constexpr int kMidMaxDeg = 1024;
 
+//   deg_begin[x] = first index whose out-degree is <= x (0 <= x <= 33), so the roots with
+//   d >= k-1 are the prefix [0, deg_begin[k-2]).
 struct RootTiers {
   vid_t* d_roots = nullptr;
   int64_t large_end = 0, mid_end = 0, small_end = 0;
+  int64_t deg_begin[34] = {0};
+  int64_t le_begin[3] = {0, 0, 0};  // first index with out-degree <= 32, 64, 128
   int min_deg = -1;  // smallest out-degree kept
 };
 
@@ -74,6 +78,8 @@ struct jgpm_graph {
   // statistics of the last count
   double last_kernel_ms = 0.0;
   int launches = 0;  // kernels launched since the counting call began
+  int tune_min_group = 4;  // narrowest lane group for the d <= 32 roots (4, 8, 16 or 32)
+  int tune_split = 128;    // roots with 32 < d <= tune_split run one per warp, above per CTA
   std::string name;
 };
 

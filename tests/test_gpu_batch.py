@@ -1,0 +1,110 @@
+"""GPU tests of the batched persistent kernel: every job's count equals its plain count and
+the oracle, alone and in the mix, under every tuning the autotuner can pick."""
+import itertools
+
+import numpy as np
+import pytest
+
+import oracle_api as O
+
+pytestmark = pytest.mark.gpu
+
+PATTERNS = ["triangle", "4-clique", "5-clique", "diamond", "4-cycle"]
+ORACLE = {"triangle": ("P0", True), "4-clique": ("P13", True), "5-clique": ("P14", True),
+          "diamond": ("P2", False), "4-cycle": ("P1", False), "6-clique": ("P15", True)}
+
+
+def mixed_graphs(J, count=12, seed=3):
+    rng = np.random.default_rng(seed)
+    specs = []
+    for j in range(count):
+        n = int(round(2 ** rng.uniform(np.log2(200), np.log2(6000))))
+        ef = int(rng.choice([4, 8, 16, 32]))
+        a = float(rng.uniform(0.45, 0.65))
+        b = c = (1 - a) / 4
+        specs.append((n, ef, a, b, c, 100 + j))
+    return specs, [J.Graph.rmat(n, ef, a, b, c, s) for (n, ef, a, b, c, s) in specs]
+
+
+@pytest.fixture(scope="module")
+def mixed(gpu):
+    specs, gs = mixed_graphs(gpu)
+    want = {}
+    for i, (n, ef, a, b, c, s) in enumerate(specs):
+        sym = O.rmat_graph(n, ef, a, b, c, s)
+        dag = O.orient(sym)
+        for p in PATTERNS + ["6-clique"]:
+            name, use_dag = ORACLE[p]
+            want[(i, p)] = O.count(name, dag if use_dag else sym)[0]
+    yield specs, gs, want
+    for g in gs:
+        g.close()
+
+
+def test_plain_counts_match_oracle(gpu, mixed):
+    specs, gs, want = mixed
+    for i, g in enumerate(gs):
+        for p in PATTERNS:
+            assert g.count(p) == want[(i, p)], (i, p)
+
+
+def test_batch_matches_plain_and_oracle(gpu, mixed):
+    specs, gs, want = mixed
+    jobs = [(g, p) for g in gs for p in PATTERNS]
+    counts, st = gpu.batch_count(jobs)
+    assert st["launches"] == 1 and st["tasks"] > 0
+    for (g, p), c in zip(jobs, counts):
+        assert c == want[(gs.index(g), p)], (gs.index(g), p)
+
+
+def test_each_job_same_alone_and_in_mix(gpu, mixed):
+    specs, gs, want = mixed
+    jobs = [(gs[i % len(gs)], PATTERNS[(i * 7) % len(PATTERNS)]) for i in range(40)]
+    counts, _ = gpu.batch_count(jobs)
+    for (g, p), c in zip(jobs, counts):
+        alone, _ = gpu.batch_count([(g, p)])
+        assert alone == [c]
+        assert c == want[(gs.index(g), p)]
+
+
+@pytest.mark.parametrize("min_group,split,rpt,isect",
+                         list(itertools.product([4, 8, 32], [8, 32], [8, 256], [0, 1])))
+def test_every_tuning_gives_the_same_counts(gpu, mixed, min_group, split, rpt, isect):
+    specs, gs, want = mixed
+    jobs = [(g, p) for g in gs[:6] for p in PATTERNS + ["6-clique"]]
+    t = gpu.Tuning(min_group, split, rpt, isect)
+    counts, st = gpu.batch_count(jobs, t)
+    assert st["tuning"]["min_group"] == min_group
+    for (g, p), c in zip(jobs, counts):
+        assert c == want[(gs.index(g), p)], (gs.index(g), p, t.as_dict())
+
+
+def test_autotune_returns_valid_tuning(gpu, mixed):
+    specs, gs, want = mixed
+    jobs = [(g, p) for g in gs for p in PATTERNS]
+    t = gpu.autotune(jobs, sample_jobs=20)
+    assert t.min_group in (4, 8, 16, 32) and t.intersect in (0, 1)
+    counts, _ = gpu.batch_count(jobs, t)
+    for (g, p), c in zip(jobs, counts):
+        assert c == want[(gs.index(g), p)]
+
+
+def test_batch_rejects_unbatchable_pattern(gpu, mixed):
+    specs, gs, want = mixed
+    with pytest.raises(gpu.JgpmError) as e:
+        gpu.batch_count([(gs[0], "P7")])
+    assert e.value.code == -5
+
+
+@pytest.mark.parametrize("min_group,split", [(4, 128), (8, 64), (32, 32), (16, 128)])
+def test_plain_tiers_any_split(gpu, mixed, min_group, split):
+    """The plain kernels' tier boundaries (lane groups, warp roots, CTA roots) do not change
+    counts on the large-degree triangle workload graph."""
+    specs, gs, want = mixed
+    g = gs[-1]
+    g.set_tuning(gpu.Tuning(min_group, split, 0, 0))
+    try:
+        for p in ("triangle", "4-clique", "5-clique"):
+            assert g.count(p) == want[(len(gs) - 1, p)]
+    finally:
+        g.set_tuning(gpu.Tuning(4, 128, 0, 0))
