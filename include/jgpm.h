@@ -194,6 +194,57 @@ int jgpm_graph_set_tuning(jgpm_graph* g, const jgpm_tuning* tuning);
  * counterpart. */
 int jgpm_autotune(const jgpm_job* jobs, int32_t njobs, int32_t sample_jobs, jgpm_tuning* out);
 
+/* ---- serving: continuous batching over a memory-budgeted graph pool -------------- */
+/* No reference counterpart (the reference runs one query per process invocation). */
+typedef struct jgpm_server jgpm_server;
+
+typedef struct {
+  uint64_t memory_budget_bytes; /* device memory for resident graphs + in-flight frontiers */
+  int32_t max_inflight;         /* batches in flight on the device at once (streams) */
+  int32_t max_batch;            /* queries packed into one batched launch */
+  int32_t device;
+  int32_t reserved;
+  jgpm_tuning tuning;           /* min_group == 0: defaults */
+} jgpm_server_config;
+
+typedef struct {
+  uint64_t submitted, completed, rejected;
+  uint64_t batches;             /* batched launches issued */
+  uint64_t evictions, restores; /* graph pool traffic */
+  uint64_t resident_bytes;      /* graph bytes resident now */
+  uint64_t peak_frontier_bytes; /* largest admitted in-flight frontier estimate */
+  double mean_batch;            /* queries per batch */
+} jgpm_server_stats;
+
+int jgpm_server_create(const jgpm_server_config* cfg, jgpm_server** s);
+
+/* Adds a graph to the pool; the server takes ownership of the handle (it frees it in
+ * jgpm_server_destroy).  The graph's DAG and root tiers are built now.  Evicted graphs keep a
+ * host copy and are uploaded again on demand (least recently used graphs go first). */
+int jgpm_server_add_graph(jgpm_server* s, jgpm_graph* g, int32_t* graph_id);
+
+/* Queues a counting query (batchable patterns, see jgpm_job) and returns its ticket at once.
+ * A query is admitted to the device when its graph is resident and its estimated frontier
+ * memory fits the budget; JGPM_EADMISSION if it can never fit. */
+int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, uint64_t* ticket);
+
+/* Waits up to timeout_ms (< 0: no limit) for a ticket; JGPM_ETIMEDOUT if it is not done. */
+int jgpm_server_wait(jgpm_server* s, uint64_t ticket, int32_t timeout_ms, uint64_t* count,
+                     double* latency_ms);
+
+int jgpm_server_get_stats(jgpm_server* s, jgpm_server_stats* st);
+
+/* Replays an open-loop trace: query i (graph_ids[i], patterns[i]) is submitted at
+ * arrival_s[i] seconds after the start, from a generator thread inside the library.
+ * mode 0 = through the server (continuous batching); mode 1 = each query as its own plain
+ * jgpm_count call, served one at a time in arrival order.  Fills counts[i] and
+ * latency_ms[i] (completion - arrival) and the wall time of the whole replay. */
+int jgpm_server_replay(jgpm_server* s, int32_t mode, int64_t n, const int32_t* graph_ids,
+                       const char* const* patterns, const double* arrival_s, uint64_t* counts,
+                       double* latency_ms, double* wall_s);
+
+int jgpm_server_destroy(jgpm_server* s);
+
 /* ---- set operations -------------------------------------------------------------- */
 #define JGPM_OP_INTERSECT 0        /* materialise {x in A & B : x < upper} */
 #define JGPM_OP_INTERSECT_COUNT 1  /* |{x in A & B : x < upper, x != exclude}| */

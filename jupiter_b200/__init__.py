@@ -25,7 +25,7 @@ __all__ = [
     "JgpmError", "Graph", "setop", "setop_batch", "solve", "lib", "library_path",
     "OP_INTERSECT", "OP_INTERSECT_COUNT", "OP_DIFFERENCE", "OP_DIFFERENCE_COUNT",
     "COUNT_STATS", "COUNT_FORCE_PLAN", "COUNT_FORCE_ENUM", "STATUS", "batch_count",
-    "autotune", "Tuning",
+    "autotune", "Tuning", "Server",
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -83,6 +83,20 @@ class _BatchStats(ctypes.Structure):
                 ("tasks", ctypes.c_int32), ("used", Tuning)]
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("memory_budget_bytes", ctypes.c_uint64), ("max_inflight", ctypes.c_int32),
+                ("max_batch", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("tuning", Tuning)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("rejected", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("evictions", ctypes.c_uint64), ("restores", ctypes.c_uint64),
+                ("resident_bytes", ctypes.c_uint64), ("peak_frontier_bytes", ctypes.c_uint64),
+                ("mean_batch", ctypes.c_double)]
+
+
 def library_path():
     return os.environ.get("JGPM_LIBRARY", os.path.join(_PKG, "libjgpm.so"))
 
@@ -133,6 +147,19 @@ def lib():
                                    _P32, _P32, _P32, _P64]
     L.jgpm_batch_count.argtypes = [ctypes.POINTER(_Job), ctypes.c_int32, ctypes.POINTER(Tuning),
                                    _PU64, ctypes.POINTER(_BatchStats)]
+    V = ctypes.c_void_p
+    L.jgpm_server_create.argtypes = [ctypes.POINTER(_ServerConfig), ctypes.POINTER(V)]
+    L.jgpm_server_add_graph.argtypes = [V, V, ctypes.POINTER(ctypes.c_int32)]
+    L.jgpm_server_submit.argtypes = [V, ctypes.c_int32, ctypes.c_char_p, _PU64]
+    L.jgpm_server_wait.argtypes = [V, ctypes.c_uint64, ctypes.c_int32, _PU64,
+                                   ctypes.POINTER(ctypes.c_double)]
+    L.jgpm_server_get_stats.argtypes = [V, ctypes.POINTER(_ServerStats)]
+    L.jgpm_server_replay.argtypes = [V, ctypes.c_int32, ctypes.c_int64, _P32,
+                                     ctypes.POINTER(ctypes.c_char_p),
+                                     ctypes.POINTER(ctypes.c_double), _PU64,
+                                     ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_double)]
+    L.jgpm_server_destroy.argtypes = [V]
     L.jgpm_graph_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
     L.jgpm_autotune.argtypes = [ctypes.POINTER(_Job), ctypes.c_int32, ctypes.c_int32,
                                 ctypes.POINTER(Tuning)]
@@ -312,6 +339,81 @@ def autotune(jobs, sample_jobs=256):
     t = Tuning()
     _check(lib().jgpm_autotune(arr, len(jobs), int(sample_jobs), ctypes.byref(t)))
     return t
+
+
+class Server:
+    """Continuous-batching query server over a memory-budgeted graph pool (one device)."""
+
+    def __init__(self, memory_budget_bytes=150 << 30, max_inflight=4, max_batch=256, device=0,
+                 tuning=None):
+        cfg = _ServerConfig()
+        cfg.memory_budget_bytes = int(memory_budget_bytes)
+        cfg.max_inflight = int(max_inflight)
+        cfg.max_batch = int(max_batch)
+        cfg.device = int(device)
+        if tuning is not None:
+            cfg.tuning = tuning
+        h = ctypes.c_void_p()
+        _check(lib().jgpm_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._graphs = []
+
+    def add_graph(self, graph):
+        """Hands the graph to the pool (the server frees it); returns its graph id."""
+        gid = ctypes.c_int32()
+        _check(lib().jgpm_server_add_graph(self._h, graph._h, ctypes.byref(gid)))
+        graph._h = ctypes.c_void_p()  # owned by the server now
+        return gid.value
+
+    def submit(self, graph_id, pattern):
+        t = ctypes.c_uint64()
+        _check(lib().jgpm_server_submit(self._h, int(graph_id), pattern.encode(),
+                                        ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        c = ctypes.c_uint64()
+        lat = ctypes.c_double()
+        _check(lib().jgpm_server_wait(self._h, int(ticket), int(timeout_ms), ctypes.byref(c),
+                                      ctypes.byref(lat)))
+        return c.value, lat.value
+
+    def stats(self):
+        st = _ServerStats()
+        _check(lib().jgpm_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _ServerStats._fields_}
+
+    def replay(self, graph_ids, patterns, arrival_s, plain=False):
+        """Open-loop trace replay inside the library; returns (counts, latency_ms, wall_s)."""
+        n = len(graph_ids)
+        gids = np.ascontiguousarray(graph_ids, dtype=np.int32)
+        arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        pats = (ctypes.c_char_p * max(n, 1))(*[p.encode() for p in patterns])
+        counts = np.zeros(max(n, 1), dtype=np.uint64)
+        lat = np.zeros(max(n, 1), dtype=np.float64)
+        wall = ctypes.c_double()
+        _check(lib().jgpm_server_replay(
+            self._h, 1 if plain else 0, n, _p32(gids), pats,
+            arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), counts.ctypes.data_as(_PU64),
+            lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(wall)))
+        return [int(x) for x in counts[:n]], lat[:n].copy(), wall.value
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().jgpm_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def setop(op, a, b, upper=None, exclude=None):

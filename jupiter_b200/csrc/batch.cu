@@ -28,53 +28,21 @@
 #include <string>
 #include <vector>
 
+#include "batch.h"
 #include "clique_dev.cuh"
 #include "jgpm_internal.h"
 #include "setops.cuh"
 
 namespace jgpm {
 
-enum BatchKind : int32_t {
-  kJobClique = 0,
-  kJobDiamond = 1,
-  kJobC4 = 2,
-};
-
-enum TaskKind : int32_t {
-  kTaskGroup4 = 0,
-  kTaskGroup8 = 1,
-  kTaskGroup16 = 2,
-  kTaskGroup32 = 3,
-  kTaskCtaRoot = 4,
-  kTaskLargeRoot = 5,
-  kTaskDiamond = 6,
-  kTaskC4 = 7,
-};
-
-struct JobDesc {
-  const eid_t* drow;  // DAG
-  const vid_t* dcol;
-  const eid_t* srow;  // symmetric
-  const vid_t* scol;
-  const vid_t* roots;  // root tiers (descending out-degree)
-  int32_t n;
-  int32_t kind;
-  int32_t k;
-  int32_t pad;
-};
-
-struct Task {
-  int32_t job;
-  int32_t kind;
-  int64_t b, e;
-};
-
 struct BatchArgs {
   const JobDesc* jobs;
-  const Task* tasks;
+  const Task* tasks;     // [0, n_c4): 4-cycle apex tasks; [n_c4, ntasks): all others
   int64_t ntasks;
+  int64_t n_c4;
+  int c4_ctas;           // CTAs [0, c4_ctas) own a dense counter array and drain the 4-cycle queue
   unsigned long long* counts;
-  unsigned long long* cursor;
+  unsigned long long* cursor;  // [0] main queue, [1] 4-cycle queue
   int dmax, W;
   int32_t* c4_counters;  // per CTA: c4_stride ints
   int64_t c4_stride;
@@ -272,12 +240,23 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs a) {
   __shared__ unsigned long long s_task;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  int32_t* c4 = a.c4_counters ? a.c4_counters + (int64_t)blockIdx.x * a.c4_stride : nullptr;
+  const bool c4_owner = a.c4_counters && (int)blockIdx.x < a.c4_ctas;
+  int32_t* c4 = c4_owner ? a.c4_counters + (int64_t)blockIdx.x * a.c4_stride : nullptr;
+  bool c4_done = !c4_owner;
   for (;;) {
-    if (tid == 0) s_task = atomicAdd(a.cursor, 1ull);
+    if (tid == 0) {
+      unsigned long long t = ~0ull;
+      if (!c4_done) {
+        t = atomicAdd(&a.cursor[1], 1ull);
+        if ((int64_t)t >= a.n_c4) t = ~0ull;
+      }
+      if (t == ~0ull) t = (unsigned long long)a.n_c4 + atomicAdd(&a.cursor[0], 1ull);
+      s_task = t;
+    }
     __syncthreads();
     const int64_t ti = (int64_t)s_task;
     __syncthreads();
+    if (ti >= a.n_c4) c4_done = true;
     if (ti >= a.ntasks) break;
     const Task t = a.tasks[ti];
     const JobDesc j = a.jobs[t.job];
@@ -303,66 +282,22 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs a) {
 // ======================================================================= host side
 namespace jgpm {
 
-int parse_batch_pattern(const char* pattern, int* kind, int* k);
-
 namespace {
 
-// Growable device buffer.
-struct DevArena {
-  void* p = nullptr;
-  size_t bytes = 0;
-  int reserve(size_t want) {
-    if (want <= bytes) return JGPM_OK;
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-    size_t sz = std::max<size_t>(want, 4096);
-    if (cudaMalloc(&p, sz) != cudaSuccess) {
-      cudaGetLastError();
-      jgpm_set_error_("batch: device allocation failed");
-      return JGPM_ENOMEM;
-    }
-    bytes = sz;
-    return JGPM_OK;
-  }
-};
-
-}  // namespace
-
-// Reusable per-device launch state of the batched kernel (task/job tables, counters,
-// scratch).  One per server slot or per synchronous caller.
-struct BatchCtx {
-  int device = 0;
-  DevArena jobs, tasks, counts, cursor, c4, lists;
-  std::vector<JobDesc> h_jobs;
-  std::vector<Task> h_tasks;
-  size_t c4_zeroed = 0;
-  ~BatchCtx() {
-    for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &lists})
-      if (d->p) cudaFree(d->p);
-  }
-};
-
-struct BatchJobIn {
-  jgpm_graph* g;
-  int kind;
-  int k;
-};
-
-static void add_range_tasks(std::vector<Task>& out, int job, int kind, int64_t b, int64_t e,
+void add_range_tasks(std::vector<Task>& out, int job, int kind, int64_t b, int64_t e,
                             int64_t chunk) {
   for (int64_t x = b; x < e; x += chunk) out.push_back(Task{job, kind, x, std::min(e, x + chunk)});
 }
 
 // Prepares every graph (DAG, root tiers) and builds the job and task tables on the host.
-static int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchCtx& c,
+int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchCtx& c,
                        int* dmax_out, int64_t* c4_n, int* max_out_deg) {
   c.h_jobs.clear();
   c.h_tasks.clear();
   int dmax = 33;
   int64_t c4max = 0;
   int maxo = 0;
-  std::vector<Task> heavy, mid, light;
+  std::vector<Task> heavy, mid, light, c4t;
   const int split = std::min(32, std::max(tu.split_degree, 4));
   for (size_t ji = 0; ji < in.size(); ++ji) {
     jgpm_graph* g = in[ji].g;
@@ -408,12 +343,14 @@ static int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu,
                       std::max<int64_t>(64, (int64_t)tu.roots_per_task * 8));
     } else {
       c4max = std::max<int64_t>(c4max, g->n);
-      add_range_tasks(mid, job, kTaskC4, 0, g->n, std::max(16, tu.roots_per_task / 4));
+      add_range_tasks(c4t, job, kTaskC4, 0, g->n, std::max(16, tu.roots_per_task / 4));
     }
     c.h_jobs.push_back(jd);
   }
   // heaviest first: large roots, then CTA roots / edge / apex chunks, then lane groups
-  c.h_tasks.reserve(heavy.size() + mid.size() + light.size());
+  c.h_tasks.reserve(c4t.size() + heavy.size() + mid.size() + light.size());
+  c.n_c4 = (int64_t)c4t.size();
+  c.h_tasks.insert(c.h_tasks.end(), c4t.begin(), c4t.end());
   c.h_tasks.insert(c.h_tasks.end(), heavy.begin(), heavy.end());
   c.h_tasks.insert(c.h_tasks.end(), mid.begin(), mid.end());
   c.h_tasks.insert(c.h_tasks.end(), light.begin(), light.end());
@@ -422,6 +359,8 @@ static int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu,
   *max_out_deg = maxo;
   return JGPM_OK;
 }
+
+}  // namespace
 
 // Enqueues one batched launch on `s`; per-job counts land in c.counts (device) and are
 // copied to `h_counts` (pinned or pageable host memory) on the same stream.
@@ -443,10 +382,12 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   if ((rc = c.jobs.reserve(nj * sizeof(JobDesc)))) return rc;
   if ((rc = c.tasks.reserve(std::max<size_t>(1, nt) * sizeof(Task)))) return rc;
   if ((rc = c.counts.reserve(nj * sizeof(unsigned long long)))) return rc;
-  if ((rc = c.cursor.reserve(sizeof(unsigned long long)))) return rc;
+  if ((rc = c.cursor.reserve(2 * sizeof(unsigned long long)))) return rc;
   BatchArgs a{};
   if (c4n > 0) {
-    const size_t need = (size_t)grid * (size_t)c4n * sizeof(int32_t);
+    const size_t per_cta = (size_t)c4n * sizeof(int32_t);
+    a.c4_ctas = (int)std::max<size_t>(1, std::min<size_t>((size_t)grid, c.c4_cap_bytes / per_cta));
+    const size_t need = (size_t)a.c4_ctas * per_cta;
     if ((rc = c.c4.reserve(need))) return rc;
     if (c.c4_zeroed < need) {  // counters are zero between apexes; zero fresh memory once
       JGPM_CUDA_TRY(cudaMemsetAsync(c.c4.p, 0, c.c4.bytes, s));
@@ -469,10 +410,11 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     JGPM_CUDA_TRY(cudaMemcpyAsync(c.tasks.p, c.h_tasks.data(), nt * sizeof(Task),
                                   cudaMemcpyHostToDevice, s));
   JGPM_CUDA_TRY(cudaMemsetAsync(c.counts.p, 0, nj * sizeof(unsigned long long), s));
-  JGPM_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, sizeof(unsigned long long), s));
+  JGPM_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, 2 * sizeof(unsigned long long), s));
   a.jobs = (const JobDesc*)c.jobs.p;
   a.tasks = (const Task*)c.tasks.p;
   a.ntasks = (int64_t)nt;
+  a.n_c4 = c.n_c4;
   a.counts = (unsigned long long*)c.counts.p;
   a.cursor = (unsigned long long*)c.cursor.p;
   a.dmax = dmax;
@@ -514,7 +456,7 @@ jgpm_tuning default_tuning() {
   return t;
 }
 
-static int collect_jobs(const jgpm_job* jobs, int32_t njobs, std::vector<BatchJobIn>& in,
+int collect_jobs(const jgpm_job* jobs, int32_t njobs, std::vector<BatchJobIn>& in,
                         int* device) {
   in.clear();
   for (int32_t i = 0; i < njobs; ++i) {

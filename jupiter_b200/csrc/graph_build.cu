@@ -585,3 +585,57 @@ int write_reference_files(const std::string& prefix, const std::vector<int64_t>&
 }
 
 }  // namespace jgpm
+
+namespace jgpm {
+
+// Frees the device arrays of a graph (CSR, DAG, tiers, scratch) and keeps a host copy of the
+// symmetric CSR so the graph can be made resident again (served graph pool eviction).
+int evict_graph(jgpm_graph* g, std::vector<int64_t>& h_rowptr, std::vector<int32_t>& h_col) {
+  if (!g->d_rowptr) return JGPM_OK;
+  if (h_rowptr.empty()) {
+    h_rowptr.resize((size_t)g->n + 1);
+    h_col.resize((size_t)g->m);
+    JGPM_CUDA_TRY(cudaMemcpyAsync(h_rowptr.data(), g->d_rowptr, ((size_t)g->n + 1) * 8,
+                                  cudaMemcpyDeviceToHost, g->stream));
+    if (g->m)
+      JGPM_CUDA_TRY(cudaMemcpyAsync(h_col.data(), g->d_col, (size_t)g->m * 4,
+                                    cudaMemcpyDeviceToHost, g->stream));
+  }
+  JGPM_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  cudaFree(g->d_rowptr);
+  cudaFree(g->d_col);
+  cudaFree(g->d_dag_rowptr);
+  cudaFree(g->d_dag_col);
+  cudaFree(g->tiers.d_roots);
+  cudaFree(g->d_scratch);
+  g->d_rowptr = nullptr;
+  g->d_col = nullptr;
+  g->d_dag_rowptr = nullptr;
+  g->d_dag_col = nullptr;
+  g->tiers = RootTiers();
+  g->d_scratch = nullptr;
+  g->scratch_bytes = 0;
+  return JGPM_OK;
+}
+
+// Uploads an evicted graph again and rebuilds its DAG and root tiers.
+int restore_graph(jgpm_graph* g, const std::vector<int64_t>& h_rowptr,
+                  const std::vector<int32_t>& h_col) {
+  if (g->d_rowptr) return JGPM_OK;
+  int rc;
+  if ((rc = upload_csr(g, h_rowptr.data(), h_col.data(), g->n, (int64_t)h_col.size(), 0)))
+    return rc;
+  if ((rc = ensure_dag(g))) return rc;
+  return ensure_tiers(g, 2);
+}
+
+// Device bytes held by a resident graph's arrays.
+uint64_t graph_device_bytes(const jgpm_graph* g) {
+  if (!g->d_rowptr) return 0;
+  uint64_t b = (uint64_t)(g->n + 1) * 8 + (uint64_t)g->m * 4;
+  if (g->d_dag_rowptr) b += (uint64_t)(g->n + 1) * 8 + (uint64_t)g->m_dag * 4;
+  if (g->tiers.d_roots) b += (uint64_t)g->n * 4;
+  return b + g->scratch_bytes;
+}
+
+}  // namespace jgpm

@@ -107,6 +107,10 @@ int ensure_control(jgpm_graph* g);
 int ensure_scratch(jgpm_graph* g, size_t bytes);
 void free_graph_device(jgpm_graph* g);
 int device_sm_count(int device);
+int evict_graph(jgpm_graph* g, std::vector<int64_t>& h_rowptr, std::vector<int32_t>& h_col);
+int restore_graph(jgpm_graph* g, const std::vector<int64_t>& h_rowptr,
+                  const std::vector<int32_t>& h_col);
+uint64_t graph_device_bytes(const jgpm_graph* g);
 // k-clique count through the bitmap kernels (capi.cu)
 int count_clique_public(jgpm_graph* g, int k, uint64_t* out, double* ms);
 // non-clique dispatch (plans.cu); *method receives a JGPM_METHOD_* code

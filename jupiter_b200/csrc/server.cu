@@ -1,0 +1,485 @@
+// Serving: continuous batching of counting queries over a memory-budgeted graph pool.
+//
+// A scheduler thread owns `max_inflight` slots (a stream, a batched-kernel context and a
+// pinned count buffer each).  Whenever a slot is free and queries are pending, it packs up to
+// `max_batch` admissible queries (FIFO) into one batched persistent launch on that slot's
+// stream and moves on; completions are detected with events, so batches of queries that
+// arrived while others run overlap on the device.  Admission: a query's graph must be
+// resident (the pool uploads it again, evicting least-recently-used idle graphs, if needed)
+// and the resident graph bytes plus the estimated frontier memory of everything in flight
+// must stay within the budget.  Counts are those of the batched kernel, i.e. exact and
+// identical to the plain per-query path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "batch.h"
+#include "jgpm_internal.h"
+
+namespace jgpm {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double now_s() {
+  return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
+}
+
+struct Query {
+  uint64_t ticket = 0;
+  int32_t graph_id = 0;
+  int kind = 0, k = 0;
+  double t_submit = 0.0, t_done = 0.0;
+  uint64_t count = 0;
+  uint64_t frontier = 0;
+  int status = 1;  // 1 pending, 0 done, < 0 error
+};
+
+struct PoolGraph {
+  jgpm_graph* g = nullptr;
+  std::vector<int64_t> h_rowptr;  // host copy once evicted
+  std::vector<int32_t> h_col;
+  uint64_t bytes = 0;             // device bytes when resident
+  uint64_t last_use = 0;
+  int inflight = 0;
+  bool resident = true;
+};
+
+struct Slot {
+  BatchCtx ctx;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done_ev = nullptr;
+  uint64_t* h_counts = nullptr;  // pinned
+  std::vector<std::shared_ptr<Query>> queries;
+  bool busy = false;
+};
+
+}  // namespace
+}  // namespace jgpm
+
+struct jgpm_server {
+  jgpm_server_config cfg;
+  std::mutex mu;
+  std::condition_variable cv_work;   // wakes the scheduler
+  std::condition_variable cv_done;   // wakes waiters
+  std::deque<std::shared_ptr<jgpm::Query>> pending;
+  std::unordered_map<uint64_t, std::shared_ptr<jgpm::Query>> tickets;
+  std::vector<jgpm::PoolGraph> graphs;
+  std::vector<std::unique_ptr<jgpm::Slot>> slots;
+  std::thread sched;
+  std::atomic<bool> stop{false};
+  uint64_t next_ticket = 1;
+  uint64_t use_clock = 0;
+  uint64_t resident_bytes = 0;
+  uint64_t inflight_frontier = 0;
+  jgpm_server_stats st{};
+  std::string sched_error;
+};
+
+namespace jgpm {
+namespace {
+
+bool over_budget(jgpm_server* s, uint64_t extra) {
+  return s->resident_bytes + s->inflight_frontier + extra > s->cfg.memory_budget_bytes;
+}
+
+// Makes graph `gid` resident, evicting idle LRU graphs while over budget (mu held).
+int make_resident(jgpm_server* s, int gid, uint64_t frontier) {
+  PoolGraph& pg = s->graphs[gid];
+  if (pg.resident) return JGPM_OK;
+  while (over_budget(s, pg.bytes + frontier)) {
+    int victim = -1;
+    for (int i = 0; i < (int)s->graphs.size(); ++i) {
+      PoolGraph& o = s->graphs[i];
+      if (i == gid || !o.resident || o.inflight > 0) continue;
+      if (victim < 0 || o.last_use < s->graphs[victim].last_use) victim = i;
+    }
+    if (victim < 0) return JGPM_EBUSY;  // try again when something completes
+    PoolGraph& v = s->graphs[victim];
+    int rc = evict_graph(v.g, v.h_rowptr, v.h_col);
+    if (rc) return rc;
+    v.resident = false;
+    s->resident_bytes -= v.bytes;
+    s->st.evictions++;
+  }
+  int rc = restore_graph(pg.g, pg.h_rowptr, pg.h_col);
+  if (rc) return rc;
+  pg.resident = true;
+  pg.bytes = graph_device_bytes(pg.g);
+  s->resident_bytes += pg.bytes;
+  s->st.restores++;
+  return JGPM_OK;
+}
+
+// Packs admissible pending queries into the free slot and launches them (mu held).
+int launch_batch(jgpm_server* s, Slot& slot) {
+  std::vector<std::shared_ptr<Query>> batch;
+  std::vector<BatchJobIn> in;
+  uint64_t frontier = 0;
+  for (auto it = s->pending.begin(); it != s->pending.end() && (int)batch.size() < s->cfg.max_batch;) {
+    std::shared_ptr<Query> q = *it;
+    PoolGraph& pg = s->graphs[q->graph_id];
+    if (!pg.resident) {
+      int rc = make_resident(s, q->graph_id, frontier + q->frontier);
+      if (rc == JGPM_EBUSY) {
+        ++it;
+        continue;
+      }
+      if (rc) return rc;
+    }
+    if (over_budget(s, frontier + q->frontier) && (!batch.empty() || s->inflight_frontier > 0)) {
+      ++it;  // wait for in-flight work to release memory
+      continue;
+    }
+    frontier += q->frontier;
+    pg.inflight++;
+    pg.last_use = ++s->use_clock;
+    in.push_back(BatchJobIn{pg.g, q->kind, q->k});
+    batch.push_back(q);
+    it = s->pending.erase(it);
+  }
+  if (batch.empty()) return JGPM_OK;
+  int ntasks = 0;
+  int rc = batch_enqueue(slot.ctx, in, s->cfg.tuning, slot.stream, slot.h_counts, &ntasks);
+  if (rc) {
+    for (auto& q : batch) {
+      q->status = rc;
+      s->graphs[q->graph_id].inflight--;
+    }
+    s->cv_done.notify_all();
+    return rc;
+  }
+  cudaEventRecord(slot.done_ev, slot.stream);
+  s->inflight_frontier += frontier;
+  s->st.peak_frontier_bytes = std::max<uint64_t>(s->st.peak_frontier_bytes, s->inflight_frontier);
+  s->st.batches++;
+  slot.queries = std::move(batch);
+  slot.busy = true;
+  return JGPM_OK;
+}
+
+void complete_slot(jgpm_server* s, Slot& slot) {
+  const double t = now_s();
+  for (size_t i = 0; i < slot.queries.size(); ++i) {
+    Query& q = *slot.queries[i];
+    q.count = slot.h_counts[i];
+    q.t_done = t;
+    q.status = 0;
+    s->graphs[q.graph_id].inflight--;
+    s->inflight_frontier -= q.frontier;
+    s->st.completed++;
+  }
+  slot.queries.clear();
+  slot.busy = false;
+}
+
+void scheduler(jgpm_server* s) {
+  cudaSetDevice(s->cfg.device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (!s->stop.load()) {
+    bool progress = false;
+    for (auto& sp : s->slots) {
+      Slot& slot = *sp;
+      if (slot.busy && cudaEventQuery(slot.done_ev) == cudaSuccess) {
+        complete_slot(s, slot);
+        progress = true;
+      }
+    }
+    if (progress) s->cv_done.notify_all();
+    for (auto& sp : s->slots) {
+      if (s->pending.empty()) break;
+      Slot& slot = *sp;
+      if (slot.busy) continue;
+      const uint64_t before = s->st.batches;
+      int rc = launch_batch(s, slot);
+      if (rc) s->sched_error = std::string(jgpm_last_error());
+      if (s->st.batches != before) progress = true;
+      else break;  // nothing admissible now
+    }
+    if (!progress) {
+      bool any_busy = false;
+      for (auto& sp : s->slots) any_busy = any_busy || sp->busy;
+      // poll completions quickly while work is in flight; otherwise sleep until a submit
+      s->cv_work.wait_for(lk, any_busy ? std::chrono::microseconds(20)
+                                       : std::chrono::milliseconds(50));
+    }
+  }
+}
+
+}  // namespace
+}  // namespace jgpm
+
+using namespace jgpm;
+
+namespace {
+
+uint64_t estimate_frontier(const jgpm_server* s, const jgpm_graph* g, int kind) {
+  const uint64_t sms = (uint64_t)device_sm_count(s->cfg.device);
+  if (kind == kJobC4) {
+    const uint64_t cap = std::max<uint64_t>((uint64_t)64 << 20,
+                                            s->cfg.memory_budget_bytes / 8 /
+                                                std::max(1, s->cfg.max_inflight));
+    return std::min<uint64_t>(cap, sms * 8 * (uint64_t)g->n * 4);
+  }
+  if (kind == kJobClique && g->tiers.large_end > 0)
+    return sms * 8 * 8 * 6 * ((uint64_t)g->max_out_degree + 32) * 4;
+  return 0;
+}
+
+int check_server(jgpm_server* s) {
+  if (!s) {
+    jgpm_set_error_("null server");
+    return JGPM_EINVAL;
+  }
+  return JGPM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int jgpm_server_create(const jgpm_server_config* cfg, jgpm_server** out) {
+  if (!cfg || !out || cfg->max_inflight < 1 || cfg->max_batch < 1 || cfg->memory_budget_bytes == 0) {
+    jgpm_set_error_("jgpm_server_create: bad config");
+    return JGPM_EINVAL;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    jgpm_set_error_("no CUDA device");
+    return JGPM_ENODEV;
+  }
+  if (cfg->device < 0 || cfg->device >= ndev) {
+    jgpm_set_error_("jgpm_server_create: no such device");
+    return JGPM_EINVAL;
+  }
+  jgpm_server* s = new jgpm_server;
+  s->cfg = *cfg;
+  if (s->cfg.tuning.min_group == 0) s->cfg.tuning = default_tuning();
+  cudaSetDevice(cfg->device);
+  const uint64_t c4cap = std::max<uint64_t>((uint64_t)64 << 20,
+                                            cfg->memory_budget_bytes / 8 / cfg->max_inflight);
+  for (int i = 0; i < cfg->max_inflight; ++i) {
+    auto sl = std::make_unique<Slot>();
+    sl->ctx.device = cfg->device;
+    sl->ctx.c4_cap_bytes = c4cap;
+    if (cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sl->done_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMallocHost((void**)&sl->h_counts, sizeof(uint64_t) * cfg->max_batch) != cudaSuccess) {
+      jgpm_set_error_("jgpm_server_create: stream/event/pinned allocation failed");
+      delete s;
+      return JGPM_ECUDA;
+    }
+    s->slots.push_back(std::move(sl));
+  }
+  s->sched = std::thread(scheduler, s);
+  *out = s;
+  return JGPM_OK;
+}
+
+int jgpm_server_add_graph(jgpm_server* s, jgpm_graph* g, int32_t* graph_id) {
+  int rc;
+  if ((rc = check_server(s))) return rc;
+  if (!g || !graph_id) {
+    jgpm_set_error_("jgpm_server_add_graph: null argument");
+    return JGPM_EINVAL;
+  }
+  if (g->device != s->cfg.device) {
+    jgpm_set_error_("jgpm_server_add_graph: graph lives on another device");
+    return JGPM_EINVAL;
+  }
+  cudaSetDevice(g->device);
+  if ((rc = ensure_dag(g)) || (rc = ensure_tiers(g, 2)) || (rc = ensure_control(g))) return rc;
+  std::unique_lock<std::mutex> lk(s->mu);
+  PoolGraph pg;
+  pg.g = g;
+  pg.bytes = graph_device_bytes(g);
+  pg.last_use = ++s->use_clock;
+  s->graphs.push_back(std::move(pg));
+  s->resident_bytes += s->graphs.back().bytes;
+  *graph_id = (int32_t)s->graphs.size() - 1;
+  // keep the pool within budget: evict idle LRU graphs (never the one just added)
+  while (s->resident_bytes > s->cfg.memory_budget_bytes) {
+    int victim = -1;
+    for (int i = 0; i + 1 < (int)s->graphs.size(); ++i) {
+      PoolGraph& o = s->graphs[i];
+      if (!o.resident || o.inflight > 0) continue;
+      if (victim < 0 || o.last_use < s->graphs[victim].last_use) victim = i;
+    }
+    if (victim < 0) break;
+    PoolGraph& v = s->graphs[victim];
+    if ((rc = evict_graph(v.g, v.h_rowptr, v.h_col))) return rc;
+    v.resident = false;
+    s->resident_bytes -= v.bytes;
+    s->st.evictions++;
+  }
+  if (s->graphs.back().bytes > s->cfg.memory_budget_bytes) {
+    jgpm_set_error_("jgpm_server_add_graph: graph alone exceeds the memory budget");
+    return JGPM_EADMISSION;
+  }
+  return JGPM_OK;
+}
+
+int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, uint64_t* ticket) {
+  int rc;
+  if ((rc = check_server(s))) return rc;
+  if (!ticket || !pattern) {
+    jgpm_set_error_("jgpm_server_submit: null argument");
+    return JGPM_EINVAL;
+  }
+  auto q = std::make_shared<Query>();
+  if (parse_batch_pattern(pattern, &q->kind, &q->k)) {
+    jgpm_set_error_(std::string("jgpm_server_submit: pattern '") + pattern +
+                    "' is not batchable");
+    return JGPM_EPATTERN;
+  }
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (graph_id < 0 || graph_id >= (int32_t)s->graphs.size()) {
+    jgpm_set_error_("jgpm_server_submit: unknown graph id");
+    return JGPM_ENOTFOUND;
+  }
+  q->graph_id = graph_id;
+  q->frontier = estimate_frontier(s, s->graphs[graph_id].g, q->kind);
+  if (q->frontier + s->graphs[graph_id].bytes > s->cfg.memory_budget_bytes) {
+    s->st.rejected++;
+    jgpm_set_error_("jgpm_server_submit: query frontier + graph exceed the memory budget");
+    return JGPM_EADMISSION;
+  }
+  q->ticket = s->next_ticket++;
+  q->t_submit = now_s();
+  s->tickets[q->ticket] = q;
+  s->pending.push_back(q);
+  s->st.submitted++;
+  *ticket = q->ticket;
+  lk.unlock();
+  s->cv_work.notify_one();
+  return JGPM_OK;
+}
+
+int jgpm_server_wait(jgpm_server* s, uint64_t ticket, int32_t timeout_ms, uint64_t* count,
+                     double* latency_ms) {
+  int rc;
+  if ((rc = check_server(s))) return rc;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) {
+    jgpm_set_error_("jgpm_server_wait: unknown ticket");
+    return JGPM_ENOTFOUND;
+  }
+  std::shared_ptr<Query> q = it->second;
+  auto ready = [&] { return q->status <= 0; };
+  if (timeout_ms < 0) {
+    s->cv_done.wait(lk, ready);
+  } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
+    jgpm_set_error_("jgpm_server_wait: timed out");
+    return JGPM_ETIMEDOUT;
+  }
+  s->tickets.erase(ticket);
+  if (q->status < 0) {
+    jgpm_set_error_("jgpm_server_wait: the batch failed: " + s->sched_error);
+    return q->status;
+  }
+  if (count) *count = q->count;
+  if (latency_ms) *latency_ms = (q->t_done - q->t_submit) * 1e3;
+  return JGPM_OK;
+}
+
+int jgpm_server_get_stats(jgpm_server* s, jgpm_server_stats* st) {
+  int rc;
+  if ((rc = check_server(s))) return rc;
+  if (!st) return JGPM_EINVAL;
+  std::unique_lock<std::mutex> lk(s->mu);
+  *st = s->st;
+  st->resident_bytes = s->resident_bytes;
+  st->mean_batch = s->st.batches ? (double)s->st.completed / (double)s->st.batches : 0.0;
+  return JGPM_OK;
+}
+
+int jgpm_server_replay(jgpm_server* s, int32_t mode, int64_t n, const int32_t* graph_ids,
+                       const char* const* patterns, const double* arrival_s, uint64_t* counts,
+                       double* latency_ms, double* wall_s) {
+  int rc;
+  if ((rc = check_server(s))) return rc;
+  if (n < 0 || (n > 0 && (!graph_ids || !patterns || !arrival_s || !counts || !latency_ms))) {
+    jgpm_set_error_("jgpm_server_replay: bad arguments");
+    return JGPM_EINVAL;
+  }
+  cudaSetDevice(s->cfg.device);
+  const double t0 = now_s();
+  auto sleep_until = [&](double t_rel) {
+    const double target = t0 + t_rel;
+    for (;;) {
+      const double d = target - now_s();
+      if (d <= 0) return;
+      if (d > 200e-6) std::this_thread::sleep_for(std::chrono::duration<double>(d - 100e-6));
+    }
+  };
+  if (mode == 0) {
+    std::vector<uint64_t> tk((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+      sleep_until(arrival_s[i]);
+      if ((rc = jgpm_server_submit(s, graph_ids[i], patterns[i], &tk[i]))) return rc;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      double lat = 0;
+      if ((rc = jgpm_server_wait(s, tk[i], -1, &counts[i], &lat))) return rc;
+      latency_ms[i] = lat;
+    }
+  } else {
+    // plain: one jgpm_count per query, in arrival order, one at a time
+    for (int64_t i = 0; i < n; ++i) {
+      sleep_until(arrival_s[i]);
+      jgpm_graph* g = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (graph_ids[i] < 0 || graph_ids[i] >= (int32_t)s->graphs.size()) return JGPM_ENOTFOUND;
+        PoolGraph& pg = s->graphs[graph_ids[i]];
+        if (!pg.resident && (rc = make_resident(s, graph_ids[i], 0))) return rc;
+        pg.last_use = ++s->use_clock;
+        pg.inflight++;
+        g = pg.g;
+      }
+      rc = jgpm_count(g, patterns[i], 0, 1, &counts[i], nullptr);
+      {
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->graphs[graph_ids[i]].inflight--;
+      }
+      if (rc) return rc;
+      latency_ms[i] = (now_s() - (t0 + arrival_s[i])) * 1e3;
+    }
+  }
+  if (wall_s) *wall_s = now_s() - t0;
+  return JGPM_OK;
+}
+
+int jgpm_server_destroy(jgpm_server* s) {
+  if (!s) return JGPM_EINVAL;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->sched.joinable()) s->sched.join();
+  for (auto& sl : s->slots) {
+    if (sl->stream) cudaStreamSynchronize(sl->stream);
+    if (sl->done_ev) cudaEventDestroy(sl->done_ev);
+    if (sl->h_counts) cudaFreeHost(sl->h_counts);
+    if (sl->stream) cudaStreamDestroy(sl->stream);
+  }
+  for (auto& pg : s->graphs) jgpm_graph_free(pg.g);
+  delete s;
+  return JGPM_OK;
+}
+
+}  // extern "C"

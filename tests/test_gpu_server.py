@@ -1,0 +1,115 @@
+"""GPU tests of the serving layer: exact counts through continuous batching, the same alone
+and in the mix; admission and the memory-budgeted pool (eviction and re-upload)."""
+import numpy as np
+import pytest
+
+import oracle_api as O
+
+pytestmark = pytest.mark.gpu
+
+PATTERNS = ["triangle", "4-clique", "5-clique", "diamond", "4-cycle"]
+ORACLE = {"triangle": ("P0", True), "4-clique": ("P13", True), "5-clique": ("P14", True),
+          "diamond": ("P2", False), "4-cycle": ("P1", False)}
+SPECS = [(1 << 12, 8, 7), (3000, 16, 8), (1 << 13, 4, 9), (1500, 32, 10)]
+
+
+@pytest.fixture(scope="module")
+def expected():
+    want = {}
+    for gi, (n, ef, seed) in enumerate(SPECS):
+        sym = O.rmat_graph(n, ef, 0.57, 0.19, 0.19, seed)
+        dag = O.orient(sym)
+        for p in PATTERNS:
+            name, use_dag = ORACLE[p]
+            want[(gi, p)] = O.count(name, dag if use_dag else sym)[0]
+    return want
+
+
+def make_server(J, budget=8 << 30, inflight=3, batch=16):
+    s = J.Server(memory_budget_bytes=budget, max_inflight=inflight, max_batch=batch)
+    ids = [s.add_graph(J.Graph.rmat(n, ef, 0.57, 0.19, 0.19, seed)) for (n, ef, seed) in SPECS]
+    return s, ids
+
+
+def test_served_counts_exact_alone_and_in_mix(gpu, expected):
+    s, ids = make_server(gpu)
+    with s:
+        # alone: one query at a time
+        alone = {}
+        for gi in ids:
+            for p in PATTERNS:
+                c, lat = s.wait(s.submit(gi, p))
+                assert c == expected[(gi, p)]
+                alone[(gi, p)] = c
+        # in the mix: many queries in flight at once, in an interleaved order
+        rng = np.random.default_rng(1)
+        qs = [(int(rng.integers(len(ids))), PATTERNS[int(rng.integers(len(PATTERNS)))])
+              for _ in range(120)]
+        tickets = [s.submit(g, p) for g, p in qs]
+        for (g, p), t in zip(qs, tickets):
+            c, lat = s.wait(t)
+            assert c == alone[(g, p)] and lat >= 0.0
+        st = s.stats()
+        assert st["completed"] == len(ids) * len(PATTERNS) + 120
+        assert st["mean_batch"] > 1.0  # queries were actually packed together
+
+
+def test_pool_evicts_and_restores_under_a_tight_budget(gpu, expected):
+    J = gpu
+    sizes = []
+    for (n, ef, seed) in SPECS:
+        with J.Graph.rmat(n, ef, 0.57, 0.19, 0.19, seed) as g:
+            g.count("triangle")  # builds the DAG and root tiers, as the pool does
+            sizes.append(g.info()["device_bytes"])
+    # room for the two largest graphs, not for all four
+    budget = sum(sorted(sizes)[-2:]) + 4096
+    s = J.Server(memory_budget_bytes=budget, max_inflight=2, max_batch=4)
+    ids = [s.add_graph(J.Graph.rmat(n, ef, 0.57, 0.19, 0.19, seed)) for (n, ef, seed) in SPECS]
+    with s:
+        for rep in range(2):
+            for gi in ids:
+                for p in ("triangle", "diamond", "4-clique"):
+                    c, _ = s.wait(s.submit(gi, p))
+                    assert c == expected[(gi, p)]
+        st = s.stats()
+        assert st["evictions"] > 0 and st["restores"] > 0
+
+
+def test_admission_rejects_what_can_never_fit(gpu):
+    J = gpu
+    s = J.Server(memory_budget_bytes=64 << 20, max_inflight=1, max_batch=4)
+    with s:
+        gid = s.add_graph(J.Graph.rmat(1 << 15, 16, 0.57, 0.19, 0.19, 3))
+        with pytest.raises(J.JgpmError) as e:
+            s.submit(gid, "4-cycle")  # dense 4-cycle counters exceed the budget
+        assert e.value.code == -11
+        assert s.stats()["rejected"] == 1
+        c, _ = s.wait(s.submit(gid, "triangle"))
+        assert c > 0
+
+
+def test_wait_timeout_and_unknown_ticket(gpu):
+    s, ids = make_server(gpu)
+    with s:
+        with pytest.raises(gpu.JgpmError) as e:
+            s.wait(123456, timeout_ms=10)
+        assert e.value.code == -12
+        with pytest.raises(gpu.JgpmError) as e:
+            s.submit(ids[0], "P7")
+        assert e.value.code == -5
+
+
+def test_replay_server_and_plain_agree(gpu, expected):
+    s, ids = make_server(gpu)
+    with s:
+        rng = np.random.default_rng(5)
+        n = 200
+        arr = np.cumsum(rng.exponential(1.0 / 2000.0, n))
+        gids = rng.integers(len(ids), size=n)
+        pats = [PATTERNS[int(x)] for x in rng.integers(len(PATTERNS), size=n)]
+        c1, lat1, w1 = s.replay(gids, pats, arr)
+        c2, lat2, w2 = s.replay(gids, pats, arr, plain=True)
+        assert c1 == c2
+        for g, p, c in zip(gids, pats, c1):
+            assert c == expected[(int(g), p)]
+        assert (lat1 >= 0).all() and (lat2 >= 0).all()
