@@ -223,7 +223,10 @@ int jgpm_server_create(const jgpm_server_config* cfg, jgpm_server** s);
  * host copy and are uploaded again on demand (least recently used graphs go first). */
 int jgpm_server_add_graph(jgpm_server* s, jgpm_graph* g, int32_t* graph_id);
 
-/* Queues a counting query (batchable patterns, see jgpm_job) and returns its ticket at once.
+/* Queues a counting query and returns its ticket at once.  Batchable patterns (see jgpm_job)
+ * are packed into batched launches; any other jgpm_count pattern runs on the server's plain
+ * lane (one jgpm_count at a time, concurrently with the batches); the prefix "induced:"
+ * (e.g. "induced:tailed-triangle") asks for the vertex-induced count.
  * A query is admitted to the device when its graph is resident and its estimated frontier
  * memory fits the budget; JGPM_EADMISSION if it can never fit. */
 int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, uint64_t* ticket);

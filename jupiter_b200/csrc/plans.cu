@@ -853,9 +853,11 @@ bool fits64(unsigned __int128 v) { return (v >> 64) == 0; }
 //   N(P4) = I(P4) + 2 I(TT) + 4 I(C4) + 6 I(D) + 12 I(K4).
 // With T = sum t_e / 3: N(diamond) = sum_e C(t_e,2); N(TT) = sum_v t_v (d_v - 2);
 // N(star) = sum_v C(d_v,3); N(P4) = sum_e (d_u-1)(d_v-1) - 3T.
-int count_census4(jgpm_graph* g, uint64_t out[6], double* ms) {
+// need_c4 = false skips the 4-cycle wedge pass; out[1] (4-path) and out[3] (4-cycle) are then
+// not computed (set to 0) -- the other four counts do not depend on N(C4).
+static int census_impl(jgpm_graph* g, uint64_t out[6], double* ms, bool need_c4) {
   Census c;
-  int rc = census_pieces(g, true, true, &c);
+  int rc = census_pieces(g, true, need_c4, &c);
   if (rc) return rc;
   typedef __int128 i128;
   const i128 T = (i128)(c.sum_te / 3);
@@ -867,7 +869,7 @@ int count_census4(jgpm_graph* g, uint64_t out[6], double* ms) {
   const i128 iTT = nTT - 4 * iD - 12 * iK4;
   const i128 iS = nS - iTT - 2 * iD - 4 * iK4;
   const i128 iP4 = nP4 - 2 * iTT - 4 * iC4 - 6 * iD - 12 * iK4;
-  const i128 v[6] = {iS, iP4, iTT, iC4, iD, iK4};
+  const i128 v[6] = {iS, need_c4 ? iP4 : 0, iTT, need_c4 ? iC4 : 0, iD, iK4};
   for (int i = 0; i < 6; ++i) {
     if (v[i] < 0) {
       jgpm_set_error_("census: negative induced count (internal inconsistency)");
@@ -881,6 +883,10 @@ int count_census4(jgpm_graph* g, uint64_t out[6], double* ms) {
   }
   if (ms) *ms = c.ms;
   return JGPM_OK;
+}
+
+int count_census4(jgpm_graph* g, uint64_t out[6], double* ms) {
+  return census_impl(g, out, ms, true);
 }
 
 // Returns JGPM_OK, a negative status, or never a method code; *method is set separately.
@@ -906,7 +912,7 @@ int count_plan_impl(jgpm_graph* g, int id, int chunk_size, unsigned flags, bool 
     *method = JGPM_METHOD_EDGE_TRIANGLE;
   } else if (id >= kIC4 && id <= kIStar3 && !force_enum) {
     uint64_t v[6];
-    if ((rc = count_census4(g, v, &t))) return rc;
+    if ((rc = census_impl(g, v, &t, id == kIC4 || id == kIPath4))) return rc;
     const int idx = id == kIStar3 ? 0 : id == kIPath4 ? 1 : id == kITailed ? 2
                   : id == kIC4 ? 3 : 4;
     cnt = v[idx];

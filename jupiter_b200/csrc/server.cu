@@ -44,6 +44,9 @@ struct Query {
   uint64_t count = 0;
   uint64_t frontier = 0;
   int status = 1;  // 1 pending, 0 done, < 0 error
+  bool plain = false;   // not batchable: runs through jgpm_count on the plain lane
+  int induced = 0;
+  std::string pattern;
 };
 
 struct PoolGraph {
@@ -74,6 +77,9 @@ struct jgpm_server {
   std::condition_variable cv_work;   // wakes the scheduler
   std::condition_variable cv_done;   // wakes waiters
   std::deque<std::shared_ptr<jgpm::Query>> pending;
+  std::deque<std::shared_ptr<jgpm::Query>> plain_pending;
+  std::condition_variable cv_plain;
+  std::thread plain_thread;
   std::unordered_map<uint64_t, std::shared_ptr<jgpm::Query>> tickets;
   std::vector<jgpm::PoolGraph> graphs;
   std::vector<std::unique_ptr<jgpm::Slot>> slots;
@@ -217,6 +223,57 @@ void scheduler(jgpm_server* s) {
   }
 }
 
+// Plain lane: queries the batched kernel does not cover (vertex-induced patterns, the
+// reference's P3..P12, ...) run one at a time through jgpm_count on their graph's stream,
+// concurrently with the batches.
+void plain_worker(jgpm_server* s) {
+  cudaSetDevice(s->cfg.device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (!s->stop.load()) {
+    if (s->plain_pending.empty()) {
+      s->cv_plain.wait_for(lk, std::chrono::milliseconds(50));
+      continue;
+    }
+    std::shared_ptr<Query> q = s->plain_pending.front();
+    PoolGraph& pg = s->graphs[q->graph_id];
+    if (!pg.resident) {
+      int rc = make_resident(s, q->graph_id, q->frontier);
+      if (rc == JGPM_EBUSY) {
+        s->cv_plain.wait_for(lk, std::chrono::microseconds(200));
+        continue;
+      }
+      if (rc) {
+        s->plain_pending.pop_front();
+        q->status = rc;
+        s->cv_done.notify_all();
+        continue;
+      }
+    }
+    if (over_budget(s, q->frontier) && s->inflight_frontier > 0) {
+      s->cv_plain.wait_for(lk, std::chrono::microseconds(200));
+      continue;
+    }
+    s->plain_pending.pop_front();
+    pg.inflight++;
+    pg.last_use = ++s->use_clock;
+    s->inflight_frontier += q->frontier;
+    jgpm_graph* g = pg.g;
+    lk.unlock();
+    uint64_t cnt = 0;
+    const int rc = jgpm_count_ex(g, q->pattern.c_str(), q->induced, 1, 0u, &cnt, nullptr);
+    const std::string err = rc ? std::string(jgpm_last_error()) : std::string();
+    lk.lock();
+    s->graphs[q->graph_id].inflight--;
+    s->inflight_frontier -= q->frontier;
+    q->count = cnt;
+    q->t_done = now_s();
+    q->status = rc;
+    if (rc) s->sched_error = err;
+    else s->st.completed++;
+    s->cv_done.notify_all();
+  }
+}
+
 }  // namespace
 }  // namespace jgpm
 
@@ -235,6 +292,14 @@ uint64_t estimate_frontier(const jgpm_server* s, const jgpm_graph* g, int kind) 
   if (kind == kJobClique && g->tiers.large_end > 0)
     return sms * 8 * 8 * 6 * ((uint64_t)g->max_out_degree + 32) * 4;
   return 0;
+}
+
+bool pattern_known(const std::string& p, int induced) {
+  if (!induced) {
+    int kind = 0, k = 0;
+    if (parse_batch_pattern(p.c_str(), &kind, &k) == JGPM_OK) return true;
+  }
+  return plan_id_of(p, induced) >= 0;
 }
 
 int check_server(jgpm_server* s) {
@@ -284,6 +349,7 @@ int jgpm_server_create(const jgpm_server_config* cfg, jgpm_server** out) {
     s->slots.push_back(std::move(sl));
   }
   s->sched = std::thread(scheduler, s);
+  s->plain_thread = std::thread(plain_worker, s);
   *out = s;
   return JGPM_OK;
 }
@@ -339,9 +405,17 @@ int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, ui
     return JGPM_EINVAL;
   }
   auto q = std::make_shared<Query>();
-  if (parse_batch_pattern(pattern, &q->kind, &q->k)) {
-    jgpm_set_error_(std::string("jgpm_server_submit: pattern '") + pattern +
-                    "' is not batchable");
+  std::string p(pattern);
+  if (p.rfind("induced:", 0) == 0) {
+    q->plain = true;
+    q->induced = 1;
+    q->pattern = p.substr(8);
+  } else if (parse_batch_pattern(pattern, &q->kind, &q->k)) {
+    q->plain = true;
+    q->pattern = p;
+  }
+  if (q->plain && !pattern_known(q->pattern, q->induced)) {
+    jgpm_set_error_(std::string("jgpm_server_submit: unknown pattern '") + pattern + "'");
     return JGPM_EPATTERN;
   }
   std::unique_lock<std::mutex> lk(s->mu);
@@ -350,7 +424,9 @@ int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, ui
     return JGPM_ENOTFOUND;
   }
   q->graph_id = graph_id;
-  q->frontier = estimate_frontier(s, s->graphs[graph_id].g, q->kind);
+  const jgpm_graph* g = s->graphs[graph_id].g;
+  q->frontier = q->plain ? (uint64_t)g->m_dag * 4 + (uint64_t)g->n * 8 + ((uint64_t)256 << 20)
+                         : estimate_frontier(s, g, q->kind);
   if (q->frontier + s->graphs[graph_id].bytes > s->cfg.memory_budget_bytes) {
     s->st.rejected++;
     jgpm_set_error_("jgpm_server_submit: query frontier + graph exceed the memory budget");
@@ -359,11 +435,13 @@ int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, ui
   q->ticket = s->next_ticket++;
   q->t_submit = now_s();
   s->tickets[q->ticket] = q;
-  s->pending.push_back(q);
+  if (q->plain) s->plain_pending.push_back(q);
+  else s->pending.push_back(q);
   s->st.submitted++;
   *ticket = q->ticket;
   lk.unlock();
-  s->cv_work.notify_one();
+  if (q->plain) s->cv_plain.notify_one();
+  else s->cv_work.notify_one();
   return JGPM_OK;
 }
 
@@ -470,7 +548,9 @@ int jgpm_server_destroy(jgpm_server* s) {
     s->stop = true;
   }
   s->cv_work.notify_all();
+  s->cv_plain.notify_all();
   if (s->sched.joinable()) s->sched.join();
+  if (s->plain_thread.joinable()) s->plain_thread.join();
   for (auto& sl : s->slots) {
     if (sl->stream) cudaStreamSynchronize(sl->stream);
     if (sl->done_ev) cudaEventDestroy(sl->done_ev);
