@@ -177,13 +177,9 @@ def run_jgpm(args):
     total_ms = sum(step_ms)
     launches = sum(x[3] for x in events)
     if world > 1:
-        tt = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-        cnt = torch.tensor([matches_step], dtype=torch.int64, device=dev)
-        dist.all_reduce(cnt)  # the one exchange: sum of the replicas' counts
-        if int(cnt.item()) != world * matches_step:
-            raise RuntimeError("replica counts disagree")
+        from jupiter_b200 import replicas
+        total_ms = replicas.max_over_ranks(total_ms, dev)
+        replicas.check_replicas([c4, c5], dev)  # the one exchange: the summed counts
     ms_per_step = total_ms / args.steps
     value = world * elems_step / (ms_per_step / 1e3)
 
@@ -219,9 +215,7 @@ def run_jgpm(args):
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
     if world > 1:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+        e2e_ms = replicas.max_over_ranks(e2e_ms, dev)
     h2d = rowptr.nbytes + col.nbytes
     d2h = 2 * 8
 
