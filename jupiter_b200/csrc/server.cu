@@ -528,7 +528,10 @@ int jgpm_server_replay(jgpm_server* s, int32_t mode, int64_t n, const int32_t* g
         pg.inflight++;
         g = pg.g;
       }
-      rc = jgpm_count(g, patterns[i], 0, 1, &counts[i], nullptr);
+      const std::string pat(patterns[i]);
+      const bool ind = pat.rfind("induced:", 0) == 0;
+      rc = jgpm_count(g, ind ? pat.c_str() + 8 : pat.c_str(), ind ? 1 : 0, 1, &counts[i],
+                      nullptr);
       {
         std::unique_lock<std::mutex> lk(s->mu);
         s->graphs[graph_ids[i]].inflight--;

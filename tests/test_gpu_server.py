@@ -95,7 +95,7 @@ def test_wait_timeout_and_unknown_ticket(gpu):
             s.wait(123456, timeout_ms=10)
         assert e.value.code == -12
         with pytest.raises(gpu.JgpmError) as e:
-            s.submit(ids[0], "P7")
+            s.submit(ids[0], "P99")
         assert e.value.code == -5
 
 
