@@ -149,6 +149,20 @@ int jgpm_count(jgpm_graph* g, const char* pattern, int induced, int chunk_size, 
 int jgpm_count_ex(jgpm_graph* g, const char* pattern, int induced, int chunk_size,
                   unsigned flags, uint64_t* out, jgpm_stats* st);
 
+/* Allocation-free count.  No counterpart in the reference: it exists for callers that may
+ * not allocate device memory while they count (a host whose own allocator holds the device,
+ * or a latency-critical path that must not call cudaMalloc/cudaFree).  It calls no
+ * cudaMalloc, cudaFree or allocating routine; the literal plan kernel's per-warp lists live
+ * in a fixed 32 MiB static device array, which limits the largest maximum degree to 262112
+ * (maximum out-degree for the DAG plans); larger graphs get JGPM_ECAPACITY.  Patterns: the
+ * reference IDs "P1".."P16", "vsgm_last_pattern" and "triangle" with induced=0, and
+ * "4-cycle", "diamond", "tailed-triangle", "4-path", "3-star" with induced=1.  The DAG plans
+ * (triangle, P13..P16) need the DAG already built (JGPM_EINVAL otherwise).  The count equals
+ * jgpm_count's.  The static arrays are shared per device: calls that overlap on one device
+ * race, so callers serialise them.  The first call on each device looks up the arrays'
+ * addresses; make it before any stream capture begins. */
+int jgpm_count_noalloc(jgpm_graph* g, const char* pattern, int induced, uint64_t* out);
+
 /* Vertex-induced census of the six connected 4-vertex graphlets, out[0..5] = 3-star,
  * 4-path, tailed triangle, 4-cycle, diamond, 4-clique. */
 int jgpm_census4(jgpm_graph* g, uint64_t out[6], jgpm_stats* st);

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "jgpm_internal.h"
@@ -958,3 +959,143 @@ int count_plan_impl(jgpm_graph* g, int id, int chunk_size, unsigned flags, bool 
 }
 
 }  // namespace jgpm
+
+// ============================================================================
+// Allocation-free counting: the literal plan kernel with its per-warp candidate lists in a
+// fixed, file-scope device array instead of memory obtained from cudaMalloc.
+//
+// Some callers cannot allocate device memory at the point where they count: a host
+// application whose own memory manager took the whole device at start-up and hands nothing
+// back, or a latency-critical path that may not call cudaMalloc/cudaFree because those calls
+// can synchronise the device and stall every other stream.  jgpm_count_noalloc serves them:
+// it calls no cudaMalloc, cudaFree or allocating library routine and works in
+// kNoAllocScratchInts int32 of scratch plus one control block, both static __device__
+// arrays.  Every GPU that loads libjgpm holds those 32 MiB until the process exits.
+namespace jgpm {
+namespace {
+
+constexpr int64_t kNoAllocScratchInts = (int64_t)8 << 20;  // 32 MiB of int32
+static __device__ __align__(256) int32_t g_noalloc_scratch[kNoAllocScratchInts];
+static __device__ __align__(256) DevControl g_noalloc_ctl;
+
+struct NoAllocDevice {
+  bool ready = false;
+  int32_t* scratch = nullptr;
+  DevControl* ctl = nullptr;
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+// Device addresses of the two arrays on the current device, looked up once per device by
+// the first call there.  In host code the array names are host-side stand-ins, not device
+// addresses, so they are never handed to a kernel directly.  The look-up can initialise the
+// module on that device, so a caller that captures streams makes its first call on each
+// device before any capture begins.
+int noalloc_setup(int device, NoAllocDevice* out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  NoAllocDevice& d = g_noalloc_dev[device];
+  if (!d.ready) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      jgpm_set_error_(std::string("jgpm_count_noalloc: cudaGetSymbolAddress(scratch): ") +
+                      cudaGetErrorString(e));
+      return JGPM_ECUDA;
+    }
+    d.scratch = static_cast<int32_t*>(p);
+    e = cudaGetSymbolAddress(&p, g_noalloc_ctl);
+    if (e != cudaSuccess) {
+      jgpm_set_error_(std::string("jgpm_count_noalloc: cudaGetSymbolAddress(control): ") +
+                      cudaGetErrorString(e));
+      return JGPM_ECUDA;
+    }
+    d.ctl = static_cast<DevControl*>(p);
+    d.ready = true;
+  }
+  *out = d;
+  return JGPM_OK;
+}
+
+}  // namespace
+}  // namespace jgpm
+
+extern "C" int jgpm_count_noalloc(jgpm_graph* g, const char* pattern, int induced,
+                                  uint64_t* out) {
+  using namespace jgpm;
+  if (!g || !pattern || !out) {
+    jgpm_set_error_("jgpm_count_noalloc: null argument");
+    return JGPM_EINVAL;
+  }
+  const std::string p(pattern);
+  const int id = p == "triangle" ? (int)kP0 : plan_id_of(p, induced);
+  if (id < 0 || id >= kNTailed) {
+    jgpm_set_error_("jgpm_count_noalloc: pattern '" + p +
+                    "' has no allocation-free plan kernel");
+    return JGPM_EPATTERN;
+  }
+  const bool dag = plan_uses_dag(id);
+  if (dag && !g->d_dag_rowptr) {
+    jgpm_set_error_("jgpm_count_noalloc: this pattern runs on the degree-oriented DAG; build it "
+                    "first (orient_dag = 1 when the graph is created, or any earlier clique "
+                    "count)");
+    return JGPM_EINVAL;
+  }
+  if (g->device < 0 || g->device >= kNoAllocMaxDevices) {
+    jgpm_set_error_("jgpm_count_noalloc: device index out of range");
+    return JGPM_EINVAL;
+  }
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != g->device) cudaSetDevice(g->device);
+  auto restore = [&]() {
+    if (prev >= 0 && prev != g->device) cudaSetDevice(prev);
+  };
+  NoAllocDevice d;
+  int rc = noalloc_setup(g->device, &d);
+  if (rc) {
+    restore();
+    return rc;
+  }
+  const int32_t maxd = dag ? g->max_out_degree : g->max_degree;
+  const int64_t cap = (int64_t)maxd + 32;
+  const int64_t per_warp = 4 * cap;
+  const int sms = device_sm_count(g->device);
+  int64_t warps = std::min<int64_t>((int64_t)sms * 64, kNoAllocScratchInts / per_warp);
+  warps -= warps % 8;
+  if (warps < 8) {
+    restore();
+    jgpm_set_error_("jgpm_count_noalloc: maximum degree " + std::to_string(maxd) +
+                    " needs more than the fixed 32 MiB scratch (largest supported maximum "
+                    "degree: " + std::to_string(kNoAllocScratchInts / 32 - 32) + ")");
+    return JGPM_ECAPACITY;
+  }
+  PlanArgs a{};
+  a.rowptr = dag ? g->d_dag_rowptr : g->d_rowptr;
+  a.col = dag ? g->d_dag_col : g->d_col;
+  a.n = g->n;
+  a.ctl = d.ctl;
+  a.scratch = d.scratch;
+  a.cap = cap;
+  a.slot_begin = 0;
+  a.slot_end = dag ? g->m_dag : g->m;
+  // The arrays keep the previous call's contents: the work cursors and the result must start
+  // at zero.  Calls that overlap on the GPU share these arrays and race.
+  cudaError_t e = cudaMemsetAsync(d.ctl, 0, sizeof(DevControl), g->stream);
+  if (e == cudaSuccess && a.slot_end > 0) {
+    rc = launch_plan(id, a, false, (int)(warps / 8), g->stream);
+    e = cudaGetLastError();
+  }
+  unsigned long long cnt = 0;
+  if (e == cudaSuccess && rc == JGPM_OK)
+    e = cudaMemcpyAsync(&cnt, &d.ctl->count[0], sizeof(cnt), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  restore();
+  if (rc) return rc;
+  if (e != cudaSuccess) {
+    jgpm_set_error_(std::string("jgpm_count_noalloc: ") + cudaGetErrorString(e));
+    return JGPM_ECUDA;
+  }
+  *out = cnt;
+  return JGPM_OK;
+}
