@@ -178,9 +178,13 @@ typedef struct {
 /* Work-split knobs of the batched kernel (and of the plain clique kernels). */
 typedef struct {
   int32_t min_group;      /* narrowest lane group for roots of out-degree <= 32: 4, 8, 16, 32 */
-  int32_t split_degree;   /* roots with out-degree above this (<= 32) run CTA-wide */
-  int32_t roots_per_task; /* roots per queued task (edges per task = 8x, apexes = 1/4x) */
-  int32_t intersect;      /* edge set ops: 0 by length ratio (merge path or search), 1 search */
+  int32_t split_degree;   /* 32, 64 or 128: roots of out-degree 32 < d <= split run one per
+                             warp, larger ones one per CTA (batched: up to out-degree 512,
+                             above that on edge-rooted lists) */
+  int32_t roots_per_task; /* lane-group roots per queued task (warp roots 1/16x, 4-cycle
+                             apexes 1/8x) */
+  int32_t intersect;      /* last clique level on edge-rooted lists: 0 searches the keys of
+                             the shorter list in the longer one, 1 always the candidates */
 } jgpm_tuning;
 
 typedef struct {

@@ -1,24 +1,34 @@
 // Batched counting: many (graph, pattern) jobs in ONE persistent, work-stealing launch.
 //
 // The reference splits one query's root-edge range into `chunk_size` static rounds, one
-// launch each (src/jupiter_gpm.cu:356-375).  Here every job of a batch is cut into tasks --
-// chunks of roots of one out-degree tier, single heavy roots, chunks of edges or of 4-cycle
-// apexes -- and all tasks of all jobs go into one global queue.  Persistent CTAs (a multiple
-// of the SM count) pull tasks with an atomic cursor until the queue is empty, so uneven
-// jobs share the GPU without host round trips; every task adds its partial count into its
-// job's counter.  Tasks are ordered heaviest first.
+// launch each (src/jupiter_gpm.cu:356-375).  Here every job of a batch is cut into tasks and
+// all tasks of all jobs go into one global queue.  Persistent CTAs pull tasks with an atomic
+// cursor until the queue is empty, so uneven jobs share the GPU without host round trips;
+// every task adds its partial count into its job's counter.  Tasks are ordered heaviest
+// first.
 //
-// Per-task work (same device code as the plain kernels, clique_dev.cuh):
-//   GROUP_G    k-clique roots with out-degree <= G, one root per G-lane group;
-//   CTA_ROOT   k-clique roots handled by the whole CTA (bitmap rows in shared memory);
-//   LARGE_ROOT k-clique roots of out-degree > 1024, edge-rooted lists in warp scratch;
-//   DIAMOND    DAG arcs (u, v): t = |N(u) & N(v)| on the symmetric lists, += C(t, 2)
-//              (the reference P2 plan, src/message_passing_gpu_kernels.cuh:188-252);
-//   C4_APEX    4-cycle apexes v0 with a per-CTA dense counter array (wedge aggregation;
-//              same count as the reference P1 plan, :104-186).
-// The tuning (jgpm_tuning) picks the narrowest lane group, the out-degree above which a root
-// runs CTA-wide, the roots per task and the edge intersection variant; jgpm_autotune picks
-// them by timing candidates on a sample of the batch.
+// Per-task work (the device code of the plain kernels, clique_dev.cuh and c4_dev.cuh):
+//   GROUP_G     k-clique roots with out-degree <= G, one root per G-lane group;
+//   WARP_ROOTS  roots with 32 < d <= split, one root per warp (bitmap in the warp's shared
+//               slice);
+//   CTA_ROOT    one root with split < d <= kBatchCtaMaxDeg on the whole CTA;
+//   LARGE_ROOT  one root with d > kBatchCtaMaxDeg, edge-rooted lists in warp scratch;
+//   C4_SMALL    4-cycle apexes with few wedges, one per warp (shared-memory hash);
+//   C4_MID      4-cycle apexes with up to 2048 wedges, each on the whole CTA (shared hash);
+//   C4_LARGE    one heavy 4-cycle apex on the whole CTA (dense counters in global memory).
+// Diamond jobs (reference P2, sum over edges of C(t_e, 2)) run the k = 3 root tasks in pair
+// mode: every triangle increments its three arcs' counters in the job's tri[] array and the
+// adds' old values give the pairs, so the count comes out of the same single pass.
+//
+// Resources: one kernel holds every task kind, so its registers and shared memory are the
+// largest any kind needs.  The CTA roots count warp-cooperatively (masks one word per lane)
+// instead of with per-thread register masks, and the per-CTA shared memory is one union of
+// the warp slices, the 4-cycle hash tables and one CTA bitmap of out-degree <= 512, so four
+// CTAs of 256 threads fit on an SM.
+//
+// The tuning (jgpm_tuning) picks the narrowest lane group, the out-degree split between warp
+// and CTA roots, and the roots per task; jgpm_autotune picks them by timing candidates on a
+// sample of the batch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,6 +39,7 @@
 #include <vector>
 
 #include "batch.h"
+#include "c4_dev.cuh"
 #include "clique_dev.cuh"
 #include "jgpm_internal.h"
 #include "setops.cuh"
@@ -37,28 +48,38 @@ namespace jgpm {
 
 struct BatchArgs {
   const JobDesc* jobs;
-  const Task* tasks;     // [0, n_c4): 4-cycle apex tasks; [n_c4, ntasks): all others
+  const Task* tasks;     // [0, n_c4): large 4-cycle apexes; [n_c4, ntasks): all others
   int64_t ntasks;
   int64_t n_c4;
-  int c4_ctas;           // CTAs [0, c4_ctas) own a dense counter array and drain the 4-cycle queue
+  int c4_ctas;           // CTAs [0, c4_ctas) own a dense counter array and drain the apex queue
   unsigned long long* counts;
-  unsigned long long* cursor;  // [0] main queue, [1] 4-cycle queue
-  int dmax, W;
-  int32_t* c4_counters;  // per CTA: c4_stride ints
+  unsigned long long* cursor;  // [0] main queue, [1] large-apex queue
+  int32_t* c4_counters;  // per owner CTA: c4_stride ints, zero between apexes
   int64_t c4_stride;
-  int32_t* list_scratch;  // per warp: 6 lists of list_cap ints
+  int32_t* list_scratch;  // per warp: kLevels lists of list_cap ints
   int64_t list_cap;
-  int intersect;  // 0 auto, 1 binary search, 2 merge path
+  int dmax, W;            // CTA-root bitmap layout
+  int intersect;          // last clique level of large roots: 0 search from the shorter list,
+                          // 1 always from the candidate list
 };
 
 namespace {
 
 constexpr int kLevels = 6;
 
+// Shared memory of one CTA of the batched kernel: the largest of the per-kind layouts.
+inline size_t batch_smem_bytes(int dmax, int W) {
+  size_t b = 8 * sizeof(WarpSmem);
+  b = std::max(b, 8 * sizeof(C4WarpHash));
+  b = std::max(b, sizeof(C4CtaHash));
+  b = std::max(b, MidLayout{dmax, W}.bytes());
+  return b;
+}
+
 template <int REM>
 struct BatchListClique {
   __device__ static acc_t run(const eid_t* rowptr, const vid_t* col, const vid_t* cand, int nc,
-                              int32_t* buf, int64_t cap) {
+                              int32_t* buf, int64_t cap, int isect) {
     const int lane = threadIdx.x & 31;
     acc_t s = 0;
     for (int i = 0; i < nc; ++i) {
@@ -66,21 +87,28 @@ struct BatchListClique {
       const eid_t b = rowptr[v];
       const int dv = (int)(rowptr[v + 1] - b);
       if (REM == 1) {
+        // |cand & N+(v)|: lanes take the keys of one list and search the other
         int c = 0;
-        for (int q = lane; q < nc; q += 32)
-          if (contains_g(col + b, dv, cand[q])) ++c;
+        if (isect == 0 && dv < nc) {
+          for (int q = lane; q < dv; q += 32)
+            if (contains_s(cand, nc, __ldg(col + b + q))) ++c;
+        } else {
+          for (int q = lane; q < nc; q += 32)
+            if (contains_g(col + b, dv, cand[q])) ++c;
+        }
         s += (acc_t)warp_sum_int(c);
       } else {
         const int t = warp_intersect_w(cand, nc, col + b, dv, INT32_MAX, buf);
         if (t > 0)
-          s += BatchListClique<(REM > 1 ? REM - 1 : 1)>::run(rowptr, col, buf, t, buf + cap, cap);
+          s += BatchListClique<(REM > 1 ? REM - 1 : 1)>::run(rowptr, col, buf, t, buf + cap, cap,
+                                                             isect);
       }
     }
     return s;
   }
 };
 
-template <int G, int K>
+template <int G, int K, bool PAIRS>
 __device__ __forceinline__ acc_t task_groups(const JobDesc& j, int64_t b, int64_t e,
                                              uint32_t* rows, int* degs) {
   constexpr int kGroups = 32 / G;
@@ -93,7 +121,7 @@ __device__ __forceinline__ acc_t task_groups(const JobDesc& j, int64_t b, int64_
   for (int64_t first = b + (int64_t)warp * kGroups; first < e; first += 8 * kGroups) {
     const int64_t idx = first + gi;
     const vid_t u = idx < e ? j.roots[idx] : -1;
-    cnt += group_root<G, K, false, false>(j.drow, j.dcol, u, R, DG, nullptr, el);
+    cnt += group_root<G, K, false, PAIRS, PAIRS>(j.drow, j.dcol, u, R, DG, j.tri, el);
   }
   return cnt;
 }
@@ -101,148 +129,121 @@ __device__ __forceinline__ acc_t task_groups(const JobDesc& j, int64_t b, int64_
 template <int G>
 __device__ __forceinline__ acc_t task_groups_k(const JobDesc& j, int64_t b, int64_t e,
                                                uint32_t* rows, int* degs) {
+  if (j.kind == kJobDiamond) return task_groups<G, 3, true>(j, b, e, rows, degs);
   switch (j.k) {
-    case 3: return task_groups<G, 3>(j, b, e, rows, degs);
-    case 4: return task_groups<G, 4>(j, b, e, rows, degs);
-    case 5: return task_groups<G, 5>(j, b, e, rows, degs);
-    case 6: return task_groups<G, 6>(j, b, e, rows, degs);
-    case 7: return task_groups<G, 7>(j, b, e, rows, degs);
-    default: return task_groups<G, 8>(j, b, e, rows, degs);
+    case 3: return task_groups<G, 3, false>(j, b, e, rows, degs);
+    case 4: return task_groups<G, 4, false>(j, b, e, rows, degs);
+    case 5: return task_groups<G, 5, false>(j, b, e, rows, degs);
+    case 6: return task_groups<G, 6, false>(j, b, e, rows, degs);
+    case 7: return task_groups<G, 7, false>(j, b, e, rows, degs);
+    default: return task_groups<G, 8, false>(j, b, e, rows, degs);
   }
 }
 
-__device__ __forceinline__ acc_t task_cta_roots(const JobDesc& j, int64_t b, int64_t e,
-                                                const MidSmem& sm) {
+template <int K, bool PAIRS>
+__device__ __forceinline__ acc_t warp_roots_k(const JobDesc& j, int64_t b, int64_t e,
+                                              WarpSmem& ws) {
   acc_t cnt = 0, el = 0;
-  for (int64_t r = b; r < e; ++r) {
-    const vid_t u = j.roots[r];
-    switch (j.k) {
-      case 3: cnt += cta_root<3, false, false>(j.drow, j.dcol, u, sm, nullptr, el); break;
-      case 4: cnt += cta_root<4, false, false>(j.drow, j.dcol, u, sm, nullptr, el); break;
-      case 5: cnt += cta_root<5, false, false>(j.drow, j.dcol, u, sm, nullptr, el); break;
-      case 6: cnt += cta_root<6, false, false>(j.drow, j.dcol, u, sm, nullptr, el); break;
-      case 7: cnt += cta_root<7, false, false>(j.drow, j.dcol, u, sm, nullptr, el); break;
-      default: cnt += cta_root<8, false, false>(j.drow, j.dcol, u, sm, nullptr, el); break;
-    }
-  }
+  for (int64_t r = b + (threadIdx.x >> 5); r < e; r += 8)
+    cnt += warp_root<K, false, PAIRS, PAIRS>(j.drow, j.dcol, j.roots[r], ws, j.tri, el);
   return cnt;
 }
 
-// Warps of the CTA take the arcs of the large roots [b, e) (edge-rooted lists).
-__device__ acc_t task_large_roots(const JobDesc& j, int64_t b, int64_t e, const BatchArgs& a) {
+__device__ __forceinline__ acc_t task_warp_roots(const JobDesc& j, int64_t b, int64_t e,
+                                                 WarpSmem& ws) {
+  if (j.kind == kJobDiamond) return warp_roots_k<3, true>(j, b, e, ws);
+  switch (j.k) {
+    case 3: return warp_roots_k<3, false>(j, b, e, ws);
+    case 4: return warp_roots_k<4, false>(j, b, e, ws);
+    case 5: return warp_roots_k<5, false>(j, b, e, ws);
+    case 6: return warp_roots_k<6, false>(j, b, e, ws);
+    case 7: return warp_roots_k<7, false>(j, b, e, ws);
+    default: return warp_roots_k<8, false>(j, b, e, ws);
+  }
+}
+
+__device__ __forceinline__ acc_t task_cta_root(const JobDesc& j, vid_t u, const MidSmem& sm) {
+  acc_t el = 0;
+  if (j.kind == kJobDiamond)
+    return cta_root<3, false, true, true, 0>(j.drow, j.dcol, u, sm, j.tri, el);
+  switch (j.k) {
+    case 3: return cta_root<3, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 4: return cta_root<4, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 5: return cta_root<5, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 6: return cta_root<6, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 7: return cta_root<7, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
+    default: return cta_root<8, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
+  }
+}
+
+// Warps of the CTA take the arcs (u, v_i) of the large root u: W = N+(u) & N+(v_i) in warp
+// scratch, then the deeper clique levels on lists (or, for diamond jobs, the pair counts of
+// the triangles (u, v_i, w)).  Returns this lane's partial.
+__device__ acc_t task_large_root(const JobDesc& j, vid_t u, const BatchArgs& a) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
   int32_t* buf = a.list_scratch + gwarp * kLevels * a.list_cap;
   const int64_t cap = a.list_cap;
+  const eid_t bu = j.drow[u];
+  const int du = (int)(j.drow[u + 1] - bu);
   acc_t cnt = 0;
-  for (int64_t r = b; r < e; ++r) {
-    const vid_t u = j.roots[r];
-    const eid_t bu = j.drow[u];
-    const int du = (int)(j.drow[u + 1] - bu);
-    for (int i = warp; i < du; i += 8) {
-      const vid_t v = __ldg(j.dcol + bu + i);
-      const eid_t bv = j.drow[v];
-      const int dv = (int)(j.drow[v + 1] - bv);
-      const int tw = warp_intersect(j.dcol + bu, du, j.dcol + bv, dv, INT32_MAX, buf);
-      if (lane == 0 && j.k == 3) cnt += (acc_t)tw;
-      if (j.k > 3 && tw > 0) {
-        acc_t c = 0;
-        switch (j.k) {
-          case 4: c = BatchListClique<1>::run(j.drow, j.dcol, buf, tw, buf + cap, cap); break;
-          case 5: c = BatchListClique<2>::run(j.drow, j.dcol, buf, tw, buf + cap, cap); break;
-          case 6: c = BatchListClique<3>::run(j.drow, j.dcol, buf, tw, buf + cap, cap); break;
-          case 7: c = BatchListClique<4>::run(j.drow, j.dcol, buf, tw, buf + cap, cap); break;
-          default: c = BatchListClique<5>::run(j.drow, j.dcol, buf, tw, buf + cap, cap); break;
-        }
-        if (lane == 0) cnt += c;
+  for (int i = warp; i < du; i += 8) {
+    const vid_t v = __ldg(j.dcol + bu + i);
+    const eid_t bv = j.drow[v];
+    const int dv = (int)(j.drow[v + 1] - bv);
+    const int tw = warp_intersect(j.dcol + bu, du, j.dcol + bv, dv, INT32_MAX, buf);
+    if (tw == 0) continue;
+    if (j.kind == kJobDiamond) {
+      if (lane == 0) cnt += pair_gain(atomicAdd(j.tri + bu + i, (unsigned)tw), (unsigned)tw);
+      for (int q = lane; q < tw; q += 32) {
+        const vid_t w = buf[q];
+        cnt += (acc_t)atomicAdd(j.tri + bu + lower_bound_g(j.dcol + bu, du, w), 1u);
+        cnt += (acc_t)atomicAdd(j.tri + bv + lower_bound_g(j.dcol + bv, dv, w), 1u);
       }
+      __syncwarp();
+      continue;
     }
+    acc_t c = (acc_t)tw;
+    const int is = a.intersect;
+    int32_t* nx = buf + cap;
+    switch (j.k) {
+      case 3: break;
+      case 4: c = BatchListClique<1>::run(j.drow, j.dcol, buf, tw, nx, cap, is); break;
+      case 5: c = BatchListClique<2>::run(j.drow, j.dcol, buf, tw, nx, cap, is); break;
+      case 6: c = BatchListClique<3>::run(j.drow, j.dcol, buf, tw, nx, cap, is); break;
+      case 7: c = BatchListClique<4>::run(j.drow, j.dcol, buf, tw, nx, cap, is); break;
+      default: c = BatchListClique<5>::run(j.drow, j.dcol, buf, tw, nx, cap, is); break;
+    }
+    if (lane == 0) cnt += c;
   }
   return cnt;
 }
 
-// DAG arcs [b, e): sum of C(|N(u) & N(v)|, 2) over the symmetric lists.
-__device__ acc_t task_diamond(const JobDesc& j, int64_t b, int64_t e, int intersect) {
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  acc_t cnt = 0;
-  for (int64_t arc = b + warp; arc < e; arc += 8) {
-    // owner u of the DAG arc
-    int64_t lo = 0, hi = j.n;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi + 1) >> 1;
-      if (j.drow[mid] <= arc) lo = mid;
-      else hi = mid - 1;
-    }
-    const vid_t u = (vid_t)lo;
-    const vid_t v = __ldg(j.dcol + arc);
-    const int32_t* Nu = j.scol + j.srow[u];
-    const int du = (int)(j.srow[u + 1] - j.srow[u]);
-    const int32_t* Nv = j.scol + j.srow[v];
-    const int dv = (int)(j.srow[v + 1] - j.srow[v]);
-    acc_t t;
-    if (intersect == 1) {
-      // binary search of the shorter list's keys in the longer list
-      const int32_t* A = du <= dv ? Nu : Nv;
-      const int32_t* B = du <= dv ? Nv : Nu;
-      const int na = min(du, dv), nb = max(du, dv);
-      int c = 0;
-      for (int q = lane; q < na; q += 32)
-        if (contains_g(B, nb, __ldg(A + q))) ++c;
-      t = (acc_t)warp_sum_int(c);
-    } else {
-      t = (acc_t)warp_intersect_count(Nu, du, Nv, dv);
-    }
-    if (lane == 0) cnt += t * (t - (t > 0 ? 1 : 0)) / 2;
-  }
-  return cnt;
+__device__ __forceinline__ acc_t task_c4_small(const JobDesc& j, int64_t b, int64_t e,
+                                               C4WarpHash& h) {
+  acc_t s = 0;
+  for (int64_t q = b + (threadIdx.x >> 5); q < e; q += 8)
+    s += c4_small_apex(j.rrow, j.rcol, j.roots[q], h);
+  return s;
 }
 
-// Apexes [b, e) of the wedge 4-cycle count; cnt_arr is this CTA's zeroed counter array.
-__device__ acc_t task_c4(const JobDesc& j, int64_t b, int64_t e, int32_t* cnt_arr) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  acc_t sum = 0;
-  for (int64_t vi = b; vi < e; ++vi) {
-    const vid_t v0 = (vid_t)vi;
-    const eid_t b0 = j.srow[v0];
-    const int64_t d0 = j.srow[v0 + 1] - b0;
-    if (d0 < 2) continue;
-    for (int pass = 0; pass < 2; ++pass) {
-      for (int64_t i = warp; i < d0; i += nw) {
-        const vid_t x = __ldg(j.scol + b0 + i);
-        const eid_t bx = j.srow[x];
-        const int64_t dx = j.srow[x + 1] - bx;
-        if (!(dx < d0 || (dx == d0 && x < v0))) continue;
-        for (int64_t q = lane; q < dx; q += 32) {
-          const vid_t v3 = __ldg(j.scol + bx + q);
-          const int64_t d3 = j.srow[v3 + 1] - j.srow[v3];
-          if (!(d3 < d0 || (d3 == d0 && v3 < v0))) continue;
-          if (pass == 0) {
-            atomicAdd(&cnt_arr[v3], 1);
-          } else {
-            const int c = atomicExch(&cnt_arr[v3], 0);
-            sum += (acc_t)c * (acc_t)(c - 1) / 2;
-          }
-        }
-      }
-      __syncthreads();
-    }
-  }
-  return sum;
-}
-
-__global__ void __launch_bounds__(256) k_batch(BatchArgs a) {
+__global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const MidSmem sm = MidSmem::carve(smem, a.dmax, a.W);
+  WarpSmem& ws = reinterpret_cast<WarpSmem*>(smem)[threadIdx.x >> 5];
+  C4WarpHash& hash = reinterpret_cast<C4WarpHash*>(smem)[threadIdx.x >> 5];
+  C4CtaHash& cta_hash = *reinterpret_cast<C4CtaHash*>(smem);
   __shared__ uint32_t rows[256];
   __shared__ int degs[256];
   __shared__ unsigned long long s_task;
+  __shared__ int s_cut;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const bool c4_owner = a.c4_counters && (int)blockIdx.x < a.c4_ctas;
   int32_t* c4 = c4_owner ? a.c4_counters + (int64_t)blockIdx.x * a.c4_stride : nullptr;
   bool c4_done = !c4_owner;
+  int smem_kind = -1;  // which layout the dynamic shared memory holds (hash tables persist)
   for (;;) {
     if (tid == 0) {
       unsigned long long t = ~0ull;
@@ -266,10 +267,30 @@ __global__ void __launch_bounds__(256) k_batch(BatchArgs a) {
       case kTaskGroup8: c = task_groups_k<8>(j, t.b, t.e, rows, degs); break;
       case kTaskGroup16: c = task_groups_k<16>(j, t.b, t.e, rows, degs); break;
       case kTaskGroup32: c = task_groups_k<32>(j, t.b, t.e, rows, degs); break;
-      case kTaskCtaRoot: c = task_cta_roots(j, t.b, t.e, sm); break;
-      case kTaskLargeRoot: c = task_large_roots(j, t.b, t.e, a); break;
-      case kTaskDiamond: c = task_diamond(j, t.b, t.e, a.intersect); break;
-      case kTaskC4: c = task_c4(j, t.b, t.e, c4); break;
+      case kTaskWarpRoots:
+        smem_kind = kTaskWarpRoots;
+        c = task_warp_roots(j, t.b, t.e, ws);
+        break;
+      case kTaskCtaRoot:
+        smem_kind = kTaskCtaRoot;
+        c = task_cta_root(j, j.roots[t.b], sm);
+        break;
+      case kTaskLargeRoot: c = task_large_root(j, j.roots[t.b], a); break;
+      case kTaskC4Small:
+        if (smem_kind != kTaskC4Small) {
+          c4_hash_init(hash);
+          smem_kind = kTaskC4Small;
+        }
+        c = task_c4_small(j, t.b, t.e, hash);
+        break;
+      case kTaskC4Mid:
+        if (smem_kind != kTaskC4Mid) {
+          c4_cta_hash_init(cta_hash);
+          smem_kind = kTaskC4Mid;
+        }
+        for (int64_t q = t.b; q < t.e; ++q) c += c4_mid_apex(j.rrow, j.rcol, j.mid[q], cta_hash);
+        break;
+      case kTaskC4Large: c = c4_large_apex(j.rrow, j.rcol, j.apexes[t.b], c4, &s_cut); break;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
     if (lane == 0 && c) atomicAdd(&a.counts[t.job], c);
@@ -285,78 +306,105 @@ namespace jgpm {
 namespace {
 
 void add_range_tasks(std::vector<Task>& out, int job, int kind, int64_t b, int64_t e,
-                            int64_t chunk) {
+                     int64_t chunk) {
   for (int64_t x = b; x < e; x += chunk) out.push_back(Task{job, kind, x, std::min(e, x + chunk)});
 }
 
-// Prepares every graph (DAG, root tiers) and builds the job and task tables on the host.
+// First index of the root tiers whose out-degree is <= x, x in {32, 64, 128, 512} (tiers
+// sorted by descending out-degree).
+int64_t tier_begin(const RootTiers& t, int x) {
+  return x <= 32 ? t.le_begin[0] : x <= 64 ? t.le_begin[1] : x <= 128 ? t.le_begin[2]
+                                                                      : t.le_begin[3];
+}
+
+struct BuildOut {
+  int dmax = 33;          // largest CTA-root out-degree
+  int64_t c4max = 0;      // largest vertex count of a job with large 4-cycle apexes
+  int max_out = 0;        // largest out-degree among the large roots
+  bool any_large = false;
+  size_t tri_bytes = 0;   // diamond counters of the batch
+};
+
+// Prepares every graph (DAG, root tiers, 4-cycle apex classes) and builds the job and task
+// tables on the host.  Diamond jobs get their per-arc counters at offsets of c.tri.
 int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchCtx& c,
-                       int* dmax_out, int64_t* c4_n, int* max_out_deg) {
+                BuildOut* o) {
   c.h_jobs.clear();
   c.h_tasks.clear();
-  int dmax = 33;
-  int64_t c4max = 0;
-  int maxo = 0;
-  std::vector<Task> heavy, mid, light, c4t;
-  const int split = std::min(32, std::max(tu.split_degree, 4));
+  std::vector<Task> heavy, cta, warp, c4m, c4s, light, c4l;
+  std::vector<size_t> tri_off(in.size(), 0);
+  const int split = tu.split_degree >= 128 ? 128 : tu.split_degree >= 64 ? 64 : 32;
+  const int64_t rpt = std::max(8, tu.roots_per_task);
   for (size_t ji = 0; ji < in.size(); ++ji) {
     jgpm_graph* g = in[ji].g;
     int rc;
-    if ((rc = ensure_dag(g))) return rc;
     JobDesc jd{};
-    jd.drow = g->d_dag_rowptr;
-    jd.dcol = g->d_dag_col;
-    jd.srow = g->d_rowptr;
-    jd.scol = g->d_col;
     jd.n = g->n;
     jd.kind = in[ji].kind;
-    jd.k = in[ji].k;
+    jd.k = in[ji].kind == kJobDiamond ? 3 : in[ji].k;
     const int job = (int)ji;
-    if (in[ji].kind == kJobClique) {
-      if ((rc = ensure_tiers(g, 2))) return rc;
-      const RootTiers& t = g->tiers;
-      jd.roots = t.d_roots;
-      const int64_t stop = t.deg_begin[in[ji].k - 2];
-      maxo = std::max(maxo, g->max_out_degree);
-      dmax = std::max(dmax, std::min(g->max_out_degree, kMidMaxDeg));
-      for (int64_t r = 0; r < std::min(stop, t.large_end); ++r)
-        heavy.push_back(Task{job, kTaskLargeRoot, r, r + 1});
-      // CTA roots: [large_end, deg_begin[split]) (out-degree above the split)
-      const int64_t cta_end = std::min(stop, std::max(t.large_end, t.deg_begin[split]));
-      for (int64_t r = t.large_end; r < cta_end; ++r) mid.push_back(Task{job, kTaskCtaRoot, r, r + 1});
-      // lane groups for d <= split
-      struct Cut { int g; int64_t b, e; };
-      const int64_t b16 = tu.min_group <= 16 ? t.deg_begin[16] : t.small_end;
-      const int64_t b8 = tu.min_group <= 8 ? t.deg_begin[8] : t.small_end;
-      const int64_t b4 = tu.min_group <= 4 ? t.deg_begin[4] : t.small_end;
-      const Cut cuts[4] = {{32, t.deg_begin[32], b16}, {16, b16, b8}, {8, b8, b4},
-                           {4, b4, t.small_end}};
-      for (const Cut& q : cuts) {
-        const int64_t b = std::max(q.b, cta_end), e = std::min(q.e, stop);
-        if (e <= b) continue;
-        const int kind = q.g == 32 ? kTaskGroup32 : q.g == 16 ? kTaskGroup16
-                       : q.g == 8 ? kTaskGroup8 : kTaskGroup4;
-        add_range_tasks(light, job, kind, b, e, std::max(8, tu.roots_per_task));
-      }
-    } else if (in[ji].kind == kJobDiamond) {
-      add_range_tasks(mid, job, kTaskDiamond, 0, g->m_dag,
-                      std::max<int64_t>(64, (int64_t)tu.roots_per_task * 8));
-    } else {
-      c4max = std::max<int64_t>(c4max, g->n);
-      add_range_tasks(c4t, job, kTaskC4, 0, g->n, std::max(16, tu.roots_per_task / 4));
+    if (in[ji].kind == kJobC4) {
+      if ((rc = ensure_c4_apexes(g))) return rc;
+      jd.rrow = g->d_rank_rowptr;
+      jd.rcol = g->d_rank_col;
+      jd.roots = g->d_c4_small;
+      jd.apexes = g->d_c4_large;
+      jd.mid = g->d_c4_mid;
+      for (int64_t q = 0; q < g->c4_nlarge; ++q) c4l.push_back(Task{job, kTaskC4Large, q, q + 1});
+      if (g->c4_nlarge > 0) o->c4max = std::max<int64_t>(o->c4max, g->n);
+      add_range_tasks(c4m, job, kTaskC4Mid, 0, g->c4_nmid, 2);
+      add_range_tasks(c4s, job, kTaskC4Small, 0, g->c4_nsmall, std::max<int64_t>(8, rpt / 8));
+      c.h_jobs.push_back(jd);
+      continue;
+    }
+    if ((rc = ensure_dag(g))) return rc;
+    if ((rc = ensure_tiers(g, 2))) return rc;
+    jd.drow = g->d_dag_rowptr;
+    jd.dcol = g->d_dag_col;
+    const RootTiers& t = g->tiers;
+    jd.roots = t.d_roots;
+    if (in[ji].kind == kJobDiamond) {
+      tri_off[ji] = o->tri_bytes;
+      o->tri_bytes += ((size_t)std::max<int64_t>(1, g->m_dag) * 4 + 255) & ~(size_t)255;
+    }
+    const int64_t stop = t.deg_begin[jd.k - 2];  // roots with d >= k-1
+    // roots by out-degree: > 512 large | (split, 512] CTA | (32, split] warp | <= 32 groups
+    const int64_t large_end = std::min(stop, tier_begin(t, kBatchCtaMaxDeg));
+    const int64_t cta_end = std::min(stop, std::max(large_end, tier_begin(t, split)));
+    const int64_t warp_end = std::min(stop, std::max(cta_end, t.deg_begin[32]));
+    for (int64_t r = 0; r < large_end; ++r) heavy.push_back(Task{job, kTaskLargeRoot, r, r + 1});
+    if (large_end > 0) {
+      o->any_large = true;
+      o->max_out = std::max(o->max_out, g->max_out_degree);
+    }
+    for (int64_t r = large_end; r < cta_end; ++r) cta.push_back(Task{job, kTaskCtaRoot, r, r + 1});
+    if (cta_end > large_end)
+      o->dmax = std::max(o->dmax, std::min(g->max_out_degree, kBatchCtaMaxDeg));
+    add_range_tasks(warp, job, kTaskWarpRoots, cta_end, warp_end, std::max<int64_t>(8, rpt / 16));
+    // lane groups for d <= 32
+    struct Cut { int g; int64_t b, e; };
+    const int64_t b16 = tu.min_group <= 16 ? t.deg_begin[16] : t.small_end;
+    const int64_t b8 = tu.min_group <= 8 ? t.deg_begin[8] : t.small_end;
+    const int64_t b4 = tu.min_group <= 4 ? t.deg_begin[4] : t.small_end;
+    const Cut cuts[4] = {{32, t.deg_begin[32], b16}, {16, b16, b8}, {8, b8, b4},
+                         {4, b4, t.small_end}};
+    for (const Cut& q : cuts) {
+      const int64_t b = std::max(q.b, warp_end), e = std::min(q.e, stop);
+      if (e <= b) continue;
+      const int kind = q.g == 32 ? kTaskGroup32 : q.g == 16 ? kTaskGroup16
+                     : q.g == 8 ? kTaskGroup8 : kTaskGroup4;
+      add_range_tasks(light, job, kind, b, e, rpt);
     }
     c.h_jobs.push_back(jd);
   }
-  // heaviest first: large roots, then CTA roots / edge / apex chunks, then lane groups
-  c.h_tasks.reserve(c4t.size() + heavy.size() + mid.size() + light.size());
-  c.n_c4 = (int64_t)c4t.size();
-  c.h_tasks.insert(c.h_tasks.end(), c4t.begin(), c4t.end());
-  c.h_tasks.insert(c.h_tasks.end(), heavy.begin(), heavy.end());
-  c.h_tasks.insert(c.h_tasks.end(), mid.begin(), mid.end());
-  c.h_tasks.insert(c.h_tasks.end(), light.begin(), light.end());
-  *dmax_out = dmax;
-  *c4_n = c4max;
-  *max_out_deg = maxo;
+  // heaviest first: large apexes (own queue), large roots, CTA roots, mid apexes, warp
+  // roots, small apexes, lane groups
+  c.n_c4 = (int64_t)c4l.size();
+  c.h_tasks.reserve(c4l.size() + heavy.size() + cta.size() + c4m.size() + warp.size() +
+                    c4s.size() + light.size());
+  for (auto* v : {&c4l, &heavy, &cta, &c4m, &warp, &c4s, &light})
+    c.h_tasks.insert(c.h_tasks.end(), v->begin(), v->end());
+  c.tri_off.swap(tri_off);
   return JGPM_OK;
 }
 
@@ -366,13 +414,12 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
 // copied to `h_counts` (pinned or pageable host memory) on the same stream.
 int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tuning& tu,
                   cudaStream_t s, uint64_t* h_counts, int* ntasks_out) {
-  int dmax = 33, maxo = 0;
-  int64_t c4n = 0;
+  BuildOut o;
   int rc;
-  if ((rc = build_tasks(in, tu, c, &dmax, &c4n, &maxo))) return rc;
+  if ((rc = build_tasks(in, tu, c, &o))) return rc;
   const int sms = device_sm_count(c.device);
-  const int W = (dmax + 31) / 32;
-  const size_t smem = MidLayout{dmax, W}.bytes();
+  const int W = (o.dmax + 31) / 32;
+  const size_t smem = batch_smem_bytes(o.dmax, W);
   cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, 256, smem);
@@ -383,9 +430,16 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   if ((rc = c.tasks.reserve(std::max<size_t>(1, nt) * sizeof(Task)))) return rc;
   if ((rc = c.counts.reserve(nj * sizeof(unsigned long long)))) return rc;
   if ((rc = c.cursor.reserve(2 * sizeof(unsigned long long)))) return rc;
+  if (o.tri_bytes) {
+    if ((rc = c.tri.reserve(o.tri_bytes))) return rc;
+    for (size_t ji = 0; ji < nj; ++ji)
+      if (c.h_jobs[ji].kind == kJobDiamond)
+        c.h_jobs[ji].tri = (uint32_t*)((char*)c.tri.p + c.tri_off[ji]);
+    JGPM_CUDA_TRY(cudaMemsetAsync(c.tri.p, 0, o.tri_bytes, s));
+  }
   BatchArgs a{};
-  if (c4n > 0) {
-    const size_t per_cta = (size_t)c4n * sizeof(int32_t);
+  if (o.c4max > 0) {
+    const size_t per_cta = (size_t)o.c4max * sizeof(int32_t);
     a.c4_ctas = (int)std::max<size_t>(1, std::min<size_t>((size_t)grid, c.c4_cap_bytes / per_cta));
     const size_t need = (size_t)a.c4_ctas * per_cta;
     if ((rc = c.c4.reserve(need))) return rc;
@@ -394,12 +448,10 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
       c.c4_zeroed = c.c4.bytes;
     }
     a.c4_counters = (int32_t*)c.c4.p;
-    a.c4_stride = c4n;
+    a.c4_stride = o.c4max;
   }
-  bool any_large = false;
-  for (const Task& t : c.h_tasks) any_large = any_large || t.kind == kTaskLargeRoot;
-  if (any_large) {
-    a.list_cap = maxo + 32;
+  if (o.any_large) {
+    a.list_cap = o.max_out + 32;
     if ((rc = c.lists.reserve((size_t)grid * 8 * kLevels * a.list_cap * sizeof(int32_t))))
       return rc;
     a.list_scratch = (int32_t*)c.lists.p;
@@ -417,7 +469,7 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   a.n_c4 = c.n_c4;
   a.counts = (unsigned long long*)c.counts.p;
   a.cursor = (unsigned long long*)c.cursor.p;
-  a.dmax = dmax;
+  a.dmax = o.dmax;
   a.W = W;
   a.intersect = tu.intersect;
   if (nt) k_batch<<<grid, 256, smem, s>>>(a);
@@ -450,7 +502,7 @@ int parse_batch_pattern(const char* pattern, int* kind, int* k) {
 jgpm_tuning default_tuning() {
   jgpm_tuning t;
   t.min_group = 8;
-  t.split_degree = 32;
+  t.split_degree = 128;
   t.roots_per_task = 256;
   t.intersect = 0;
   return t;
@@ -599,8 +651,8 @@ int jgpm_autotune(const jgpm_job* jobs, int32_t njobs, int32_t sample_jobs, jgpm
   double best_ms = measure(best);
   // coordinate descent over the four knobs
   const int groups[] = {4, 8, 16, 32};
-  const int splits[] = {8, 16, 32};
-  const int rpt[] = {32, 128, 512, 2048};
+  const int splits[] = {32, 64, 128};
+  const int rpt[] = {64, 256, 1024, 4096};
   const int isect[] = {0, 1};
   for (int pass = 0; pass < 2 && rc == JGPM_OK; ++pass) {
     for (int gsz : groups) {

@@ -16,22 +16,31 @@ enum BatchKind : int32_t {
 };
 
 enum TaskKind : int32_t {
-  kTaskGroup4 = 0,
+  kTaskGroup4 = 0,     // roots [b, e) of out-degree <= 4 .. 32, one per lane group
   kTaskGroup8 = 1,
   kTaskGroup16 = 2,
   kTaskGroup32 = 3,
-  kTaskCtaRoot = 4,
-  kTaskLargeRoot = 5,
-  kTaskDiamond = 6,
-  kTaskC4 = 7,
+  kTaskWarpRoots = 4,  // roots [b, e) of out-degree 32 < d <= split, one per warp
+  kTaskCtaRoot = 5,    // root b, split < d <= kBatchCtaMaxDeg, the whole CTA
+  kTaskLargeRoot = 6,  // root b, d > kBatchCtaMaxDeg, warps take its arcs (edge-rooted lists)
+  kTaskC4Small = 7,    // small 4-cycle apexes [b, e) of the job's list, one per warp
+  kTaskC4Large = 8,    // large 4-cycle apex b of the job's list, the whole CTA
+  kTaskC4Mid = 9,      // mid 4-cycle apexes [b, e) of the job's list, one after another per CTA
 };
 
+// Out-degree above which a batched root runs on the edge-rooted list path (the CTA bitmap of
+// a root of out-degree d takes about 20 d + d^2 / 8 bytes of shared memory).
+constexpr int kBatchCtaMaxDeg = 512;
+
 struct JobDesc {
-  const eid_t* drow;  // DAG
+  const eid_t* drow;    // DAG (cliques, diamond)
   const vid_t* dcol;
-  const eid_t* srow;  // symmetric
-  const vid_t* scol;
-  const vid_t* roots;  // root tiers (descending out-degree)
+  const eid_t* rrow;    // rank-relabelled symmetric CSR (4-cycle)
+  const vid_t* rcol;
+  const vid_t* roots;   // root tiers (descending out-degree), or the small 4-cycle apexes
+  const vid_t* apexes;  // large 4-cycle apexes (descending wedge bound)
+  const vid_t* mid;     // mid 4-cycle apexes
+  uint32_t* tri;        // diamond: per-arc triangle counters (zero at launch)
   int32_t n;
   int32_t kind;
   int32_t k;
@@ -68,14 +77,15 @@ struct DevArena {
 // scratch).  One per server slot or per synchronous caller.
 struct BatchCtx {
   int device = 0;
-  DevArena jobs, tasks, counts, cursor, c4, lists;
+  DevArena jobs, tasks, counts, cursor, c4, lists, tri;
   std::vector<JobDesc> h_jobs;
   std::vector<Task> h_tasks;
   int64_t n_c4 = 0;
+  std::vector<size_t> tri_off;  // diamond jobs: offset of the job's counters in `tri`
   size_t c4_zeroed = 0;
   size_t c4_cap_bytes = (size_t)4 << 30;  // memory cap of the 4-cycle counter arrays
   ~BatchCtx() {
-    for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &lists})
+    for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &lists, &tri})
       if (d->p) cudaFree(d->p);
   }
 };

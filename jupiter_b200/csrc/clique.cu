@@ -44,10 +44,12 @@ struct CliqueArgs {
   uint32_t* tri;        // edge-triangle mode: triangles per DAG arc (K == 3 only)
 };
 
+// Kernel variants: PAIRS (with ETRI, K == 3) returns sum_e C(t_e, 2) as the count.
+
 namespace {
 
 // ------------------------------------------------------------------ small tiers (d <= 32)
-template <int G, int K, bool STATS, bool ETRI = false>
+template <int G, int K, bool STATS, bool ETRI = false, bool PAIRS = false>
 __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
   __shared__ uint32_t rows_s[256];
   __shared__ int deg_s[256];
@@ -66,7 +68,7 @@ __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
     if (first >= a.end) break;
     const int64_t idx = first + gi;
     const vid_t u = idx < a.end ? a.roots[idx] : -1;
-    cnt += group_root<G, K, STATS, ETRI>(a.rowptr, a.col, u, R, DG, a.tri, elems);
+    cnt += group_root<G, K, STATS, ETRI, PAIRS>(a.rowptr, a.col, u, R, DG, a.tri, elems);
   }
   for (int o = 16; o > 0; o >>= 1) {
     cnt += __shfl_xor_sync(kFull, cnt, o);
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
 }
 
 // ------------------------------------------------------------------ warp tier (d <= 128)
-template <int K, bool STATS, bool ETRI = false>
+template <int K, bool STATS, bool ETRI = false, bool PAIRS = false>
 __global__ void __launch_bounds__(256) k_clique_warp(CliqueArgs a) {
   extern __shared__ __align__(16) unsigned char wsmem[];
   WarpSmem& ws = reinterpret_cast<WarpSmem*>(wsmem)[threadIdx.x >> 5];
@@ -91,7 +93,7 @@ __global__ void __launch_bounds__(256) k_clique_warp(CliqueArgs a) {
     c0 = __shfl_sync(kFull, c0, 0);
     const int64_t idx = a.begin + (int64_t)c0;
     if (idx >= a.end) break;
-    cnt += warp_root<K, STATS, ETRI>(a.rowptr, a.col, a.roots[idx], ws, a.tri, elems);
+    cnt += warp_root<K, STATS, ETRI, PAIRS>(a.rowptr, a.col, a.roots[idx], ws, a.tri, elems);
   }
   for (int o = 16; o > 0; o >>= 1) {
     cnt += __shfl_xor_sync(kFull, cnt, o);
@@ -104,7 +106,7 @@ __global__ void __launch_bounds__(256) k_clique_warp(CliqueArgs a) {
 }
 
 // ------------------------------------------------------------------ mid tier (d <= 1024)
-template <int K, bool STATS, bool ETRI = false>
+template <int K, bool STATS, bool ETRI = false, bool PAIRS = false>
 __global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int W) {
   extern __shared__ __align__(16) unsigned char smem[];
   const MidSmem sm = MidSmem::carve(smem, dmax, W);
@@ -118,7 +120,7 @@ __global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int 
     const int64_t idx = (int64_t)s_idx + a.begin;
     __syncthreads();
     if (idx >= a.end) break;
-    cnt += cta_root<K, STATS, ETRI>(a.rowptr, a.col, a.roots[idx], sm, a.tri, elems);
+    cnt += cta_root<K, STATS, ETRI, PAIRS>(a.rowptr, a.col, a.roots[idx], sm, a.tri, elems);
   }
   for (int o = 16; o > 0; o >>= 1) {
     cnt += __shfl_xor_sync(kFull, cnt, o);
@@ -162,7 +164,7 @@ struct ListClique {
   }
 };
 
-template <int K, bool STATS, bool ETRI = false>
+template <int K, bool STATS, bool ETRI = false, bool PAIRS = false>
 __global__ void __launch_bounds__(256) k_clique_large(CliqueArgs a) {
   const int lane = threadIdx.x & 31;
   const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -198,19 +200,25 @@ __global__ void __launch_bounds__(256) k_clique_large(CliqueArgs a) {
     const int dv = (int)(a.rowptr[v + 1] - bv);
     int32_t* W = buf;
     const int tw = warp_intersect(a.col + bu, du, a.col + bv, dv, INT32_MAX, W);
+    // tw and the ListClique sums are the same in every lane: lane 0 keeps them
     if (K == 3) {
-      cnt += (acc_t)tw;
+      if (!PAIRS && lane == 0) cnt += (acc_t)tw;
       if (ETRI && tw > 0) {
-        if (lane == 0) atomicAdd(a.tri + bu + i, (unsigned)tw);
+        if (lane == 0) {
+          const unsigned o = atomicAdd(a.tri + bu + i, (unsigned)tw);
+          if (PAIRS) cnt += pair_gain(o, (unsigned)tw);
+        }
         for (int q = lane; q < tw; q += 32) {
           const vid_t w = W[q];
-          atomicAdd(a.tri + bu + lower_bound_g(a.col + bu, du, w), 1u);
-          atomicAdd(a.tri + bv + lower_bound_g(a.col + bv, dv, w), 1u);
+          const unsigned o1 = atomicAdd(a.tri + bu + lower_bound_g(a.col + bu, du, w), 1u);
+          const unsigned o2 = atomicAdd(a.tri + bv + lower_bound_g(a.col + bv, dv, w), 1u);
+          if (PAIRS) cnt += (acc_t)o1 + (acc_t)o2;
         }
         __syncwarp();
       }
     } else if (tw > 0) {
-      cnt += ListClique<(K > 3 ? K - 3 : 1), STATS>::run(a, W, tw, buf + cap, cap, elems);
+      const acc_t c = ListClique<(K > 3 ? K - 3 : 1), STATS>::run(a, W, tw, buf + cap, cap, elems);
+      if (lane == 0) cnt += c;
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -252,7 +260,7 @@ struct TierPlan {
   TierRange large, mid, warp, g32, g16, g8, g4;
 };
 
-template <int K, bool STATS, bool ETRI>
+template <int K, bool STATS, bool ETRI, bool PAIRS = false>
 int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream_t s,
                   int mid_dmax) {
   CliqueArgs a = base;
@@ -261,7 +269,7 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     a.begin = p.large.b;
     a.end = p.large.e;
     a.cursor = 2;
-    k_clique_large<K, STATS, ETRI><<<sms * 2, 256, 0, s>>>(a);
+    k_clique_large<K, STATS, ETRI, PAIRS><<<sms * 2, 256, 0, s>>>(a);
     ++n;
   }
   if (!p.mid.empty()) {
@@ -270,13 +278,13 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     a.cursor = 1;
     const int W = (mid_dmax + 31) / 32;
     const size_t sm = MidLayout{mid_dmax, W}.bytes();
-    cudaFuncSetAttribute(k_clique_mid<K, STATS, ETRI>,
+    cudaFuncSetAttribute(k_clique_mid<K, STATS, ETRI, PAIRS>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clique_mid<K, STATS, ETRI>, 256,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clique_mid<K, STATS, ETRI, PAIRS>, 256,
                                                   sm);
     if (per_sm < 1) per_sm = 1;
-    k_clique_mid<K, STATS, ETRI><<<sms * per_sm, 256, sm, s>>>(a, mid_dmax, W);
+    k_clique_mid<K, STATS, ETRI, PAIRS><<<sms * per_sm, 256, sm, s>>>(a, mid_dmax, W);
     ++n;
   }
   if (!p.warp.empty()) {
@@ -284,13 +292,13 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     a.end = p.warp.e;
     a.cursor = 7;
     const size_t sm = 8 * sizeof(WarpSmem);
-    cudaFuncSetAttribute(k_clique_warp<K, STATS, ETRI>,
+    cudaFuncSetAttribute(k_clique_warp<K, STATS, ETRI, PAIRS>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clique_warp<K, STATS, ETRI>, 256,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clique_warp<K, STATS, ETRI, PAIRS>, 256,
                                                   sm);
     if (per_sm < 1) per_sm = 1;
-    k_clique_warp<K, STATS, ETRI><<<sms * per_sm, 256, sm, s>>>(a);
+    k_clique_warp<K, STATS, ETRI, PAIRS><<<sms * per_sm, 256, sm, s>>>(a);
     ++n;
   }
   const TierRange* gr[4] = {&p.g32, &p.g16, &p.g8, &p.g4};
@@ -300,10 +308,10 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     a.end = gr[q]->e;
     a.cursor = 3 + q;
     switch (q) {
-      case 0: k_clique_group<32, K, STATS, ETRI><<<sms * 8, 256, 0, s>>>(a); break;
-      case 1: k_clique_group<16, K, STATS, ETRI><<<sms * 8, 256, 0, s>>>(a); break;
-      case 2: k_clique_group<8, K, STATS, ETRI><<<sms * 8, 256, 0, s>>>(a); break;
-      default: k_clique_group<4, K, STATS, ETRI><<<sms * 8, 256, 0, s>>>(a); break;
+      case 0: k_clique_group<32, K, STATS, ETRI, PAIRS><<<sms * 8, 256, 0, s>>>(a); break;
+      case 1: k_clique_group<16, K, STATS, ETRI, PAIRS><<<sms * 8, 256, 0, s>>>(a); break;
+      case 2: k_clique_group<8, K, STATS, ETRI, PAIRS><<<sms * 8, 256, 0, s>>>(a); break;
+      default: k_clique_group<4, K, STATS, ETRI, PAIRS><<<sms * 8, 256, 0, s>>>(a); break;
     }
     ++n;
   }
@@ -344,7 +352,7 @@ static TierPlan make_plan(const RootTiers& t, int k, int64_t root_begin, int64_t
 // >= 2 into elements[0] when stats); tri != null selects the edge-triangle mode (k = 3).
 // The caller zeroes the work cursors before each call.
 int launch_clique_ex(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64_t root_end,
-                     cudaStream_t s, uint32_t* tri, int min_group) {
+                     cudaStream_t s, uint32_t* tri, int min_group, bool pairs = false) {
   if (k < 3 || k > 8) {
     jgpm_set_error_("k-clique: k must be in [3, 8]");
     return JGPM_EPATTERN;
@@ -370,7 +378,8 @@ int launch_clique_ex(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64
   const int mid_dmax = std::max(33, std::min(g->max_out_degree, kMidMaxDeg));
   int n = 0;
   if (tri) {
-    n = launch_plan_k<3, false, true>(a, p, sms, s, mid_dmax);
+    n = pairs ? launch_plan_k<3, false, true, true>(a, p, sms, s, mid_dmax)
+              : launch_plan_k<3, false, true>(a, p, sms, s, mid_dmax);
   } else {
     switch (k) {
 #define JGPM_K(KK)                                                              \
@@ -404,6 +413,17 @@ int launch_edge_triangles(jgpm_graph* g, uint32_t* d_tri, cudaStream_t s) {
   if ((rc = ensure_control(g))) return rc;
   JGPM_CUDA_TRY(cudaMemsetAsync(g->d_ctl, 0, sizeof(DevControl), s));
   return launch_clique_ex(g, 3, false, 0, g->tiers.small_end, s, d_tri, g->tune_min_group);
+}
+
+// Diamond count sum_e C(t_e, 2) into ctl->count[0] in one pass; d_tri (m_dag counters) must
+// be zero on entry.
+int launch_diamond_pairs(jgpm_graph* g, uint32_t* d_tri, cudaStream_t s) {
+  int rc;
+  if ((rc = ensure_tiers(g, 2))) return rc;
+  if ((rc = ensure_control(g))) return rc;
+  JGPM_CUDA_TRY(cudaMemsetAsync(g->d_ctl, 0, sizeof(DevControl), s));
+  return launch_clique_ex(g, 3, false, 0, g->tiers.small_end, s, d_tri, g->tune_min_group,
+                          true);
 }
 
 // Level-1 set-op elements of the edge-rooted plan into g->d_ctl->elements[1].

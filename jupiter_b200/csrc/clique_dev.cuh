@@ -5,11 +5,23 @@
 //     R_i bit j  <=>  L[j] in N+(L[i])
 // are the level-1 sets of the reference's edge-rooted plans (W of arc (u, L[i]));
 // K_k(u) = sum_i C_{k-3}(R_i) with C_0(m) = popc(m), C_t(m) = sum_{j in m} C_{t-1}(m & R_j).
+//
+// Modes of the k = 3 root kernels:
+//   ETRI   every triangle adds one to each of its three DAG arcs in tri[] (edge triangles);
+//   PAIRS  ETRI whose adds return the old value; an add of k to a counter holding o creates
+//          k*o + C(k, 2) new pairs of triangles on that edge, so the sum over all adds is
+//          sum_e C(t_e, 2) -- the diamond count -- in one pass (tri[] starts at zero).
+//   The root kernels return the pair count in PAIRS mode and the clique count otherwise.
 #pragma once
 #include "jgpm_internal.h"
 #include "setops.cuh"
 
 namespace jgpm {
+
+// Pairs of triangles created on one edge by adding k to a counter that held o.
+__device__ __forceinline__ acc_t pair_gain(unsigned o, unsigned k) {
+  return (acc_t)k * (acc_t)o + (acc_t)k * (acc_t)(k - 1) / 2;
+}
 
 constexpr int kRangeCut = 32;  // restrict a row to [L0, Ld-1] when longer than this
 
@@ -43,7 +55,7 @@ struct SmallCount<0, STATS> {
 // with its group's root u (or u < 0 for an idle group).  R and DG point at the group's G
 // shared words.  Returns this lane's partial count.  tri (edge-triangle mode) receives one
 // count per triangle arc.
-template <int G, int K, bool STATS, bool ETRI>
+template <int G, int K, bool STATS, bool ETRI, bool PAIRS = false>
 __device__ __forceinline__ acc_t group_root(const eid_t* __restrict__ rowptr,
                                             const vid_t* __restrict__ col, vid_t u,
                                             uint32_t* R, int* DG, uint32_t* tri,
@@ -73,6 +85,7 @@ __device__ __forceinline__ acc_t group_root(const eid_t* __restrict__ rowptr,
     }
   }
   R[gl] = 0u;
+  if (ETRI) DG[gl] = 0;  // column counts (DG is free when STATS is off)
   int off = len;  // inclusive scan of the row lengths within the group
 #pragma unroll
   for (int o = 1; o < G; o <<= 1) {
@@ -82,6 +95,7 @@ __device__ __forceinline__ acc_t group_root(const eid_t* __restrict__ rowptr,
   const int T = __shfl_sync(kFull, off, G - 1, G);
   const int Tmax = (G == 32) ? T : (int)__reduce_max_sync(kFull, (unsigned)T);
   const int row_start = off - len;
+  acc_t pairs = 0;
   __syncwarp();
   for (int t0 = 0; t0 < Tmax; t0 += G) {
     const int t = t0 + gl;
@@ -104,18 +118,26 @@ __device__ __forceinline__ acc_t group_root(const eid_t* __restrict__ rowptr,
     const vid_t lp = __shfl_sync(kFull, Lj, p, G);
     if (t < T && lp == x) {
       atomicOr(&R[i], 1u << p);
-      if (ETRI) {  // triangle (u, L[i], L[p]): one count on each of its three arcs
-        atomicAdd(tri + si + (t - sti), 1u);
-        atomicAdd(tri + base + i, 1u);
-        atomicAdd(tri + base + p, 1u);
+      if (ETRI) {  // triangle (u, L[i], L[p]): the arc L[i] -> L[p] gets its count now
+        const unsigned o = atomicAdd(tri + si + (t - sti), 1u);
+        if (PAIRS) pairs += (acc_t)o;
+        atomicAdd(&DG[p], 1);
       }
     }
   }
   __syncwarp();
   acc_t cnt = 0;
-  if (gl < d) cnt = SmallCount<K - 3, STATS>::run(R[gl], R, DG, elems);
+  if (!PAIRS && gl < d) cnt = SmallCount<K - 3, STATS>::run(R[gl], R, DG, elems);
+  if (ETRI && gl < d) {
+    // the root's own arc (u, L[gl]) lies on popc(R_gl) + (rows with bit gl) triangles
+    const unsigned tu = (unsigned)__popc(R[gl]) + (unsigned)DG[gl];
+    if (tu) {
+      const unsigned o = atomicAdd(tri + base + gl, tu);
+      if (PAIRS) pairs += pair_gain(o, tu);
+    }
+  }
   __syncwarp();
-  return cnt;
+  return PAIRS ? pairs : cnt;
 }
 
 // ---------------------------------------------------------------- multi-word rows
@@ -218,9 +240,10 @@ struct WarpSmem {
   int deg[kWarpMaxDeg];
   eid_t rs[kWarpMaxDeg];
   uint32_t R[kWarpMaxDeg * kWarpW];
+  int colcnt[kWarpMaxDeg];  // edge-triangle mode: rows with bit j set
 };
 
-template <int K, bool STATS, bool ETRI>
+template <int K, bool STATS, bool ETRI, bool PAIRS = false>
 __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
                                            const vid_t* __restrict__ col, vid_t u, WarpSmem& ws,
                                            uint32_t* tri, acc_t& elems) {
@@ -230,6 +253,8 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
   const int w_d = (d + 31) >> 5;
   for (int j = lane; j < d; j += 32) ws.L[j] = __ldg(col + base + j);
   for (int q = lane; q < d * w_d; q += 32) ws.R[q] = 0u;
+  if (ETRI)
+    for (int q = lane; q < d; q += 32) ws.colcnt[q] = 0;
   __syncwarp();
   const vid_t lo_key = ws.L[0], hi_key = ws.L[d - 1];
   for (int i = lane; i < d; i += 32) {
@@ -268,6 +293,7 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
     __syncwarp();
   }
   const int T = ws.off[d];
+  acc_t pairs = 0;
   for (int t = lane; t < T; t += 32) {
     int lo = 0, hi = d - 1;  // row i: last i with off[i] <= t
     while (lo < hi) {
@@ -286,9 +312,9 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
     if (p0 < d && ws.L[p0] == x) {
       atomicOr(&ws.R[i * w_d + (p0 >> 5)], 1u << (p0 & 31));
       if (ETRI) {
-        atomicAdd(tri + ws.rs[i] + (t - ws.off[i]), 1u);
-        atomicAdd(tri + base + i, 1u);
-        atomicAdd(tri + base + p0, 1u);
+        const unsigned o = atomicAdd(tri + ws.rs[i] + (t - ws.off[i]), 1u);
+        if (PAIRS) pairs += (acc_t)o;
+        atomicAdd(&ws.colcnt[p0], 1);
       }
     }
   }
@@ -298,10 +324,19 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
     uint32_t m[kWarpW];
 #pragma unroll
     for (int q = 0; q < kWarpW; ++q) m[q] = q < w_d ? ws.R[i * w_d + q] : 0u;
-    cnt += RowCount<K - 3, kWarpW, STATS>::run(m, ws.R, w_d, ws.deg, elems);
+    if (!PAIRS) cnt += RowCount<K - 3, kWarpW, STATS>::run(m, ws.R, w_d, ws.deg, elems);
+    if (ETRI) {
+      unsigned tu = (unsigned)ws.colcnt[i];
+#pragma unroll
+      for (int q = 0; q < kWarpW; ++q) tu += (unsigned)__popc(m[q]);
+      if (tu) {
+        const unsigned o = atomicAdd(tri + base + i, tu);
+        if (PAIRS) pairs += pair_gain(o, tu);
+      }
+    }
   }
   __syncwarp();
-  return cnt;
+  return PAIRS ? pairs : cnt;
 }
 
 // Shared layout for one mid-tier root (dynamic shared memory):
@@ -339,8 +374,9 @@ struct MidSmem {
 constexpr int kCtaRowWords = 16;
 
 // One root of out-degree 32 < d <= dmax processed by the whole CTA (blockDim = 256).
-// Every thread calls it; returns this thread's partial count.
-template <int K, bool STATS, bool ETRI>
+// Every thread calls it; returns this thread's partial count.  Rows of up to ROWW words are
+// counted row-parallel from registers, wider ones (or all, with ROWW = 0) warp-cooperatively.
+template <int K, bool STATS, bool ETRI, bool PAIRS = false, int ROWW = kCtaRowWords>
 __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
                                           const vid_t* __restrict__ col, vid_t u,
                                           const MidSmem& sm, uint32_t* tri, acc_t& elems) {
@@ -365,7 +401,7 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
     const vid_t v = L[i];
     eid_t s = rowptr[v];
     int len = (int)(rowptr[v + 1] - s);
-    deg[i] = len;
+    deg[i] = ETRI ? 0 : len;  // edge-triangle mode reuses deg[] as column counts
     if (len > kRangeCut) {
       const int lb = lower_bound_g(col + s, len, lo_key);
       const int ub = upper_bound_g(col + s, len, hi_key);
@@ -402,6 +438,7 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
     __syncthreads();
   }
   const int T = off[d];
+  acc_t pairs = 0;
   for (int t = tid; t < T; t += nthreads) {
     int lo = 0, hi = d - 1;  // row i: last i with off[i] <= t
     while (lo < hi) {
@@ -420,21 +457,36 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
     if (p0 < d && L[p0] == x) {
       atomicOr(&R[(size_t)i * w_d + (p0 >> 5)], 1u << (p0 & 31));
       if (ETRI) {
-        atomicAdd(tri + rs[i] + (t - off[i]), 1u);
-        atomicAdd(tri + base + i, 1u);
-        atomicAdd(tri + base + p0, 1u);
+        const unsigned o = atomicAdd(tri + rs[i] + (t - off[i]), 1u);
+        if (PAIRS) pairs += (acc_t)o;
+        atomicAdd(&deg[p0], 1);
       }
     }
   }
   __syncthreads();
+  if (ETRI) {  // the root's own arcs: popc(R_i) + (rows with bit i) triangles each
+    for (int i = tid; i < d; i += nthreads) {
+      unsigned tu = (unsigned)deg[i];
+      for (int q = 0; q < w_d; ++q) tu += (unsigned)__popc(R[(size_t)i * w_d + q]);
+      if (tu) {
+        const unsigned o = atomicAdd(tri + base + i, tu);
+        if (PAIRS) pairs += pair_gain(o, tu);
+      }
+    }
+  }
+  if (PAIRS) {
+    __syncthreads();
+    return pairs;
+  }
   acc_t cnt = 0;
-  if (w_d <= kCtaRowWords) {
+  constexpr int RW = ROWW > 0 ? ROWW : 1;
+  if (ROWW > 0 && w_d <= ROWW) {
     // row-parallel: each thread owns rows, masks in registers
     for (int i = tid; i < d; i += nthreads) {
-      uint32_t m[kCtaRowWords];
+      uint32_t m[RW];
 #pragma unroll
-      for (int q = 0; q < kCtaRowWords; ++q) m[q] = q < w_d ? R[(size_t)i * w_d + q] : 0u;
-      cnt += RowCount<K - 3, kCtaRowWords, STATS>::run(m, R, w_d, deg, elems);
+      for (int q = 0; q < RW; ++q) m[q] = q < w_d ? R[(size_t)i * w_d + q] : 0u;
+      cnt += RowCount<K - 3, RW, STATS>::run(m, R, w_d, deg, elems);
     }
   } else {
     // very wide rows: the mask is distributed one word per lane

@@ -479,8 +479,8 @@ int ensure_tiers(jgpm_graph* g, int min_deg) {
     }
     g->tiers.deg_begin[x] = lo;
   }
-  const uint32_t le_thr[3] = {32u, 64u, 128u};
-  for (int q = 0; q < 3; ++q) {
+  const uint32_t le_thr[4] = {32u, 64u, 128u, 512u};
+  for (int q = 0; q < 4; ++q) {
     int64_t lo = 0, hi = g->tiers.small_end;
     while (lo < hi) {
       const int64_t mid = (lo + hi) >> 1;
@@ -513,16 +513,119 @@ int ensure_scratch(jgpm_graph* g, size_t bytes) {
   return JGPM_OK;
 }
 
+int ensure_aux(jgpm_graph* g, size_t bytes) {
+  if (g->aux_bytes >= bytes) return JGPM_OK;
+  if (g->d_aux) cudaFree(g->d_aux);
+  g->d_aux = nullptr;
+  g->aux_bytes = 0;
+  int rc;
+  if ((rc = dalloc((char**)&g->d_aux, bytes))) return rc;
+  g->aux_bytes = bytes;
+  return JGPM_OK;
+}
+
 void free_graph_device(jgpm_graph* g) {
   cudaFree(g->d_rowptr);
   cudaFree(g->d_col);
   cudaFree(g->d_dag_rowptr);
   cudaFree(g->d_dag_col);
+  cudaFree(g->d_rank_rowptr);
+  cudaFree(g->d_rank_col);
+  cudaFree(g->d_c4_small);
+  cudaFree(g->d_c4_mid);
+  cudaFree(g->d_c4_large);
   cudaFree(g->tiers.d_roots);
   cudaFree(g->d_ctl);
   cudaFree(g->d_scratch);
+  cudaFree(g->d_aux);
   if (g->h_ctl) cudaFreeHost(g->h_ctl);
   if (g->stream) cudaStreamDestroy(g->stream);
+}
+
+}  // namespace jgpm
+
+// ------------------------------------------------------------------- rank relabelling
+namespace jgpm {
+namespace {
+
+__global__ void k_rank_keys(const int64_t* rowptr, int32_t n, uint64_t* keys, int32_t* vals) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    keys[v] = ((uint64_t)(rowptr[v + 1] - rowptr[v]) << 32) | (uint64_t)v;
+    vals[v] = (int32_t)v;
+  }
+}
+
+__global__ void k_invert(const int32_t* order, int32_t n, int32_t* rank) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride)
+    rank[order[p]] = (int32_t)p;
+}
+
+__global__ void k_rank_arc_keys(const int32_t* src, const int32_t* col, const int32_t* rank,
+                                int64_t m, int shift, uint64_t* keys) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride)
+    keys[k] = ((uint64_t)rank[src[k]] << shift) | (uint64_t)rank[col[k]];
+}
+
+__global__ void k_low_bits(const uint64_t* keys, int64_t m, uint64_t mask, int32_t* col) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride)
+    col[k] = (int32_t)(keys[k] & mask);
+}
+
+}  // namespace
+
+// Relabels the symmetric CSR by rank -- position in (degree, id) order, the order the DAG
+// orientation uses -- and sorts every row by rank, so "neighbours ranked below v" is a prefix
+// of each row.  Built once per graph.
+int ensure_rank_csr(jgpm_graph* g) {
+  if (g->d_rank_rowptr) return JGPM_OK;
+  cudaStream_t s = g->stream;
+  const int32_t n = g->n;
+  const int64_t m = g->m;
+  const int shift = shift_for(n);
+  int rc;
+  DevBuf k0, k1, v0, v1, rank, src, tmp;
+  if ((rc = dalloc((uint64_t**)&k0.p, n))) return rc;
+  if ((rc = dalloc((uint64_t**)&k1.p, n))) return rc;
+  if ((rc = dalloc((int32_t**)&v0.p, n))) return rc;
+  if ((rc = dalloc((int32_t**)&v1.p, n))) return rc;
+  if ((rc = dalloc((int32_t**)&rank.p, n))) return rc;
+  k_rank_keys<<<grid_for(n), 256, 0, s>>>(g->d_rowptr, n, (uint64_t*)k0.p, (int32_t*)v0.p);
+  size_t tb = 0;
+  JGPM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t*)k0.p, (uint64_t*)k1.p,
+                                                (int32_t*)v0.p, (int32_t*)v1.p, n, 0, 64, s));
+  if ((rc = dalloc((char**)&tmp.p, tb))) return rc;
+  JGPM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp.p, tb, (uint64_t*)k0.p, (uint64_t*)k1.p,
+                                                (int32_t*)v0.p, (int32_t*)v1.p, n, 0, 64, s));
+  k_invert<<<grid_for(n), 256, 0, s>>>((int32_t*)v1.p, n, (int32_t*)rank.p);
+  // arcs as (rank(u), rank(v)) keys, sorted
+  DevBuf ak, ak2, tmp2;
+  if ((rc = dalloc((int32_t**)&src.p, m))) return rc;
+  if ((rc = dalloc((uint64_t**)&ak.p, m))) return rc;
+  if ((rc = dalloc((uint64_t**)&ak2.p, m))) return rc;
+  k_arc_src<<<grid_for((int64_t)n * 32), 256, 0, s>>>(g->d_rowptr, n, (int32_t*)src.p);
+  k_rank_arc_keys<<<grid_for(m), 256, 0, s>>>((int32_t*)src.p, g->d_col, (int32_t*)rank.p, m,
+                                              shift, (uint64_t*)ak.p);
+  cub::DoubleBuffer<uint64_t> db((uint64_t*)ak.p, (uint64_t*)ak2.p);
+  size_t tb2 = 0;
+  JGPM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb2, db, m, 0, 2 * shift, s));
+  if ((rc = dalloc((char**)&tmp2.p, tb2))) return rc;
+  JGPM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(tmp2.p, tb2, db, m, 0, 2 * shift, s));
+  if ((rc = dalloc(&g->d_rank_rowptr, (size_t)n + 1))) return rc;
+  if ((rc = dalloc(&g->d_rank_col, m))) {
+    cudaFree(g->d_rank_rowptr);
+    g->d_rank_rowptr = nullptr;
+    return rc;
+  }
+  k_low_bits<<<grid_for(m), 256, 0, s>>>(db.Current(), m, (1ull << shift) - 1, g->d_rank_col);
+  k_rowptr_from_keys<<<grid_for((int64_t)n + 1), 256, 0, s>>>(db.Current(), m, n, shift,
+                                                              g->d_rank_rowptr);
+  JGPM_CUDA_TRY(cudaGetLastError());
+  JGPM_CUDA_TRY(cudaStreamSynchronize(s));
+  return JGPM_OK;
 }
 
 }  // namespace jgpm
@@ -606,8 +709,24 @@ int evict_graph(jgpm_graph* g, std::vector<int64_t>& h_rowptr, std::vector<int32
   cudaFree(g->d_col);
   cudaFree(g->d_dag_rowptr);
   cudaFree(g->d_dag_col);
+  cudaFree(g->d_rank_rowptr);
+  cudaFree(g->d_rank_col);
+  cudaFree(g->d_c4_small);
+  cudaFree(g->d_c4_mid);
+  cudaFree(g->d_c4_large);
   cudaFree(g->tiers.d_roots);
   cudaFree(g->d_scratch);
+  cudaFree(g->d_aux);
+  g->d_aux = nullptr;
+  g->aux_bytes = 0;
+  g->d_rank_rowptr = nullptr;
+  g->d_rank_col = nullptr;
+  g->d_c4_small = nullptr;
+  g->d_c4_mid = nullptr;
+  g->d_c4_large = nullptr;
+  g->c4_nsmall = -1;
+  g->c4_nmid = 0;
+  g->c4_nlarge = 0;
   g->d_rowptr = nullptr;
   g->d_col = nullptr;
   g->d_dag_rowptr = nullptr;
@@ -635,7 +754,9 @@ uint64_t graph_device_bytes(const jgpm_graph* g) {
   uint64_t b = (uint64_t)(g->n + 1) * 8 + (uint64_t)g->m * 4;
   if (g->d_dag_rowptr) b += (uint64_t)(g->n + 1) * 8 + (uint64_t)g->m_dag * 4;
   if (g->tiers.d_roots) b += (uint64_t)g->n * 4;
-  return b + g->scratch_bytes;
+  if (g->d_rank_rowptr) b += (uint64_t)(g->n + 1) * 8 + (uint64_t)g->m * 4;
+  if (g->d_c4_small) b += (uint64_t)(g->c4_nsmall + g->c4_nmid + g->c4_nlarge) * 4 + 48;
+  return b + g->scratch_bytes + g->aux_bytes;
 }
 
 }  // namespace jgpm

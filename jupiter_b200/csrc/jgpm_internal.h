@@ -34,7 +34,7 @@ struct RootTiers {
   vid_t* d_roots = nullptr;
   int64_t large_end = 0, mid_end = 0, small_end = 0;
   int64_t deg_begin[34] = {0};
-  int64_t le_begin[3] = {0, 0, 0};  // first index with out-degree <= 32, 64, 128
+  int64_t le_begin[4] = {0, 0, 0, 0};  // first index with out-degree <= 32, 64, 128, 512
   int min_deg = -1;  // smallest out-degree kept
 };
 
@@ -68,6 +68,18 @@ struct jgpm_graph {
   int64_t m_dag = 0;
   int64_t* d_dag_rowptr = nullptr;
   int32_t* d_dag_col = nullptr;
+  // rank-relabelled symmetric CSR (vertex ids replaced by their (degree, id) rank, rows sorted
+  // by rank), built on demand for the 4-cycle wedge count
+  int64_t* d_rank_rowptr = nullptr;
+  int32_t* d_rank_col = nullptr;
+  // 4-cycle apexes of the rank CSR by wedge bound (built on demand): one-warp, one-CTA
+  // shared-memory and dense-counter classes, the last sorted by descending bound
+  int32_t* d_c4_small = nullptr;
+  int32_t* d_c4_mid = nullptr;
+  int32_t* d_c4_large = nullptr;
+  int64_t c4_nsmall = -1;  // -1 = not built
+  int64_t c4_nmid = 0;
+  int64_t c4_nlarge = 0;
   int32_t max_out_degree = 0;
   jgpm::RootTiers tiers;
   // per-graph reusable launch state
@@ -75,6 +87,8 @@ struct jgpm_graph {
   jgpm::DevControl* h_ctl = nullptr;  // pinned mirror
   void* d_scratch = nullptr;          // per-CTA scratch for heavy roots
   size_t scratch_bytes = 0;
+  void* d_aux = nullptr;              // per-arc counters (edge triangles, diamond pairs)
+  size_t aux_bytes = 0;
   // statistics of the last count
   double last_kernel_ms = 0.0;
   int launches = 0;  // kernels launched since the counting call began
@@ -102,9 +116,14 @@ int rmat_build(jgpm_graph* g, int64_t n, int64_t num_edges, double a, double b, 
 int upload_csr(jgpm_graph* g, const int64_t* rowptr, const int32_t* col, int32_t n, int64_t m,
                int validate);
 int ensure_dag(jgpm_graph* g);
+int ensure_rank_csr(jgpm_graph* g);
+// c4.cu: apex classes of the 4-cycle count (needs the rank CSR)
+int ensure_c4_apexes(jgpm_graph* g);
+int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms);
 int ensure_tiers(jgpm_graph* g, int min_deg);
 int ensure_control(jgpm_graph* g);
 int ensure_scratch(jgpm_graph* g, size_t bytes);
+int ensure_aux(jgpm_graph* g, size_t bytes);
 void free_graph_device(jgpm_graph* g);
 int device_sm_count(int device);
 int evict_graph(jgpm_graph* g, std::vector<int64_t>& h_rowptr, std::vector<int32_t>& h_col);

@@ -36,6 +36,7 @@ namespace jgpm {
 int launch_clique(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64_t root_end,
                   cudaStream_t s);
 int launch_edge_triangles(jgpm_graph* g, uint32_t* d_tri, cudaStream_t s);
+int launch_diamond_pairs(jgpm_graph* g, uint32_t* d_tri, cudaStream_t s);
 
 enum PlanId {
   kP0 = 0, kP1 = 1, kP2 = 2, kP3 = 3, kP4 = 4, kP5 = 5, kP6 = 6, kP7 = 7, kP8 = 8, kP9 = 9,
@@ -501,56 +502,6 @@ __global__ void __launch_bounds__(256) k_plan(PlanArgs a) {
   }
 }
 
-// ------------------------------------------------------------------ wedge 4-cycle count
-// CTA per apex v0 (highest rank); a dense per-CTA counter array of n ints in global scratch
-// (all zero between apexes).
-__device__ __forceinline__ bool rank_less(const eid_t* rowptr, vid_t a, int64_t da, vid_t b,
-                                          int64_t db) {
-  return da < db || (da == db && a < b);
-}
-
-__global__ void __launch_bounds__(256) k_wedge_c4(const eid_t* rowptr, const vid_t* col,
-                                                  vid_t n, DevControl* ctl, int32_t* counters,
-                                                  int64_t vbegin, int64_t vend) {
-  int32_t* cnt = counters + (int64_t)blockIdx.x * n;
-  __shared__ unsigned long long s_v;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  acc_t sum = 0;
-  for (;;) {
-    if (tid == 0) s_v = atomicAdd(&ctl->counter[0], 1ull);
-    __syncthreads();
-    const int64_t vi = (int64_t)s_v + vbegin;
-    __syncthreads();
-    if (vi >= vend) break;
-    const vid_t v0 = (vid_t)vi;
-    const eid_t b0 = rowptr[v0];
-    const int64_t d0 = rowptr[v0 + 1] - b0;
-    if (d0 < 2) continue;
-    for (int pass = 0; pass < 2; ++pass) {
-      for (int64_t i = warp; i < d0; i += nw) {
-        const vid_t x = __ldg(col + b0 + i);
-        const eid_t bx = rowptr[x];
-        const int64_t dx = rowptr[x + 1] - bx;
-        if (!rank_less(rowptr, x, dx, v0, d0)) continue;
-        for (int64_t j = lane; j < dx; j += 32) {
-          const vid_t v3 = __ldg(col + bx + j);
-          const int64_t d3 = rowptr[v3 + 1] - rowptr[v3];
-          if (!rank_less(rowptr, v3, d3, v0, d0)) continue;
-          if (pass == 0) {
-            atomicAdd(&cnt[v3], 1);
-          } else {
-            const int c = atomicExch(&cnt[v3], 0);
-            sum += (acc_t)c * (acc_t)(c - 1) / 2;
-          }
-        }
-      }
-      __syncthreads();
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
-  if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
-}
-
 // ------------------------------------------------------------------ census reductions
 struct U128 {
   unsigned long long lo, hi;
@@ -734,34 +685,25 @@ int run_literal(jgpm_graph* g, int id, int chunk_size, bool stats, uint64_t* out
   return JGPM_OK;
 }
 
+// The 4-cycle count runs on the rank-relabelled CSR (c4.cu); rounds do not change it.
 int run_wedge_c4(jgpm_graph* g, int chunk_size, uint64_t* out, double* ms) {
+  (void)chunk_size;
+  return count_c4_wedge(g, out, ms);
+}
+
+// Diamond count (reference P2 semantics) in one pass over the DAG's triangles: every
+// increment of an edge's triangle counter from o to o + k adds k*o + C(k, 2) to the total, so
+// the total is sum_e C(t_e, 2).  Per-arc counters live in g->d_aux.
+int run_diamond_pairs(jgpm_graph* g, uint64_t* out, double* ms) {
   int rc;
-  if ((rc = ensure_control(g))) return rc;
-  const int sms = device_sm_count(g->device);
-  const int64_t per_cta = (int64_t)g->n;
-  int64_t ctas = std::min<int64_t>((int64_t)sms * 2, ((int64_t)8 << 30) / (per_cta * 4));
-  ctas = std::max<int64_t>(1, ctas);
-  const size_t bytes = (size_t)(ctas * per_cta) * sizeof(int32_t);
-  if ((rc = ensure_scratch(g, bytes))) return rc;
-  JGPM_CUDA_TRY(cudaMemsetAsync(g->d_scratch, 0, bytes, g->stream));
-  JGPM_CUDA_TRY(cudaMemsetAsync(g->d_ctl, 0, sizeof(DevControl), g->stream));
-  const int rounds = chunk_size > 1 ? chunk_size : 1;
-  const int64_t per = ((int64_t)g->n + rounds - 1) / rounds;
+  if ((rc = ensure_dag(g))) return rc;
+  const size_t bytes = (size_t)std::max<int64_t>(1, g->m_dag) * sizeof(uint32_t);
+  if ((rc = ensure_aux(g, bytes))) return rc;
   Timer t;
   cudaEventRecord(t.a, g->stream);
-  for (int r = 0; r < rounds; ++r) {
-    const int64_t b = std::min<int64_t>(g->n, (int64_t)r * per);
-    const int64_t e = std::min<int64_t>(g->n, b + per);
-    if (r > 0)
-      JGPM_CUDA_TRY(cudaMemsetAsync(g->d_ctl->counter, 0, sizeof(g->d_ctl->counter), g->stream));
-    if (e > b) {
-      k_wedge_c4<<<(int)ctas, 256, 0, g->stream>>>(g->d_rowptr, g->d_col, g->n, g->d_ctl,
-                                                   (int32_t*)g->d_scratch, b, e);
-      ++g->launches;
-    }
-  }
+  JGPM_CUDA_TRY(cudaMemsetAsync(g->d_aux, 0, bytes, g->stream));
+  if ((rc = launch_diamond_pairs(g, (uint32_t*)g->d_aux, g->stream))) return rc;
   cudaEventRecord(t.b, g->stream);
-  JGPM_CUDA_TRY(cudaGetLastError());
   if ((rc = read_ctl(g))) return rc;
   *out = g->h_ctl->count[0];
   if (ms) *ms = t.ms();
@@ -785,30 +727,17 @@ int census_pieces(jgpm_graph* g, bool need_k4, bool need_c4, Census* c) {
   if ((rc = ensure_control(g))) return rc;
   cudaStream_t s = g->stream;
   memset(c, 0, sizeof(*c));
-  uint32_t* d_tri = nullptr;
-  unsigned long long* d_tv2 = nullptr;
-  unsigned long long* d_acc = nullptr;
+  // per-arc triangles | twice the triangles per vertex | 16 accumulator words, in g->d_aux
+  const size_t tri_bytes = ((size_t)std::max<int64_t>(1, g->m_dag) * 4 + 255) & ~(size_t)255;
+  const size_t tv2_bytes = (size_t)std::max<int32_t>(1, g->n) * 8;
+  if ((rc = ensure_aux(g, tri_bytes + tv2_bytes + 16 * 8))) return rc;
+  uint32_t* d_tri = (uint32_t*)g->d_aux;
+  unsigned long long* d_tv2 = (unsigned long long*)((char*)g->d_aux + tri_bytes);
+  unsigned long long* d_acc = d_tv2 + std::max<int32_t>(1, g->n);
   Timer t;
   cudaEventRecord(t.a, s);
-  auto cleanup = [&]() {
-    cudaFree(d_tri);
-    cudaFree(d_tv2);
-    cudaFree(d_acc);
-  };
-  if (cudaMalloc(&d_tri, std::max<int64_t>(1, g->m_dag) * sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&d_tv2, std::max<int64_t>(1, g->n) * sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&d_acc, 16 * sizeof(unsigned long long)) != cudaSuccess) {
-    cleanup();
-    jgpm_set_error_("census: device allocation failed");
-    return JGPM_ENOMEM;
-  }
-  cudaMemsetAsync(d_tri, 0, std::max<int64_t>(1, g->m_dag) * sizeof(uint32_t), s);
-  cudaMemsetAsync(d_tv2, 0, std::max<int64_t>(1, g->n) * sizeof(unsigned long long), s);
-  cudaMemsetAsync(d_acc, 0, 16 * sizeof(unsigned long long), s);
-  if ((rc = launch_edge_triangles(g, d_tri, s))) {
-    cleanup();
-    return rc;
-  }
+  JGPM_CUDA_TRY(cudaMemsetAsync(g->d_aux, 0, tri_bytes + tv2_bytes + 16 * 8, s));
+  if ((rc = launch_edge_triangles(g, d_tri, s))) return rc;
   k_census_edges<<<grid_for((int64_t)g->n * 32), 256, 0, s>>>(
       g->d_dag_rowptr, g->d_dag_col, g->d_rowptr, g->n, d_tri, d_tv2, d_acc);
   k_census_vertices<<<grid_for(g->n), 256, 0, s>>>(g->d_rowptr, g->n, d_tv2, d_acc);
@@ -817,11 +746,9 @@ int census_pieces(jgpm_graph* g, bool need_k4, bool need_c4, Census* c) {
   cudaEventRecord(t.b, s);
   if (cudaMemcpyAsync(h, d_acc, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess) {
-    cleanup();
     jgpm_set_error_(std::string("census: ") + cudaGetErrorString(cudaGetLastError()));
     return JGPM_ECUDA;
   }
-  cleanup();
   double ms = t.ms();
   c->sum_te = u128(&h[0]);
   c->sum_c2 = u128(&h[2]);
@@ -902,14 +829,7 @@ int count_plan_impl(jgpm_graph* g, int id, int chunk_size, unsigned flags, bool 
     if ((rc = run_wedge_c4(g, chunk_size, &cnt, &t))) return rc;
     *method = JGPM_METHOD_WEDGE;
   } else if (id == kP2 && !force_plan) {
-    Census c;
-    if ((rc = census_pieces(g, false, false, &c))) return rc;
-    if (!fits64(c.sum_c2)) {
-      jgpm_set_error_("diamond count exceeds uint64");
-      return JGPM_EOVERFLOW;
-    }
-    cnt = (uint64_t)c.sum_c2;
-    t = c.ms;
+    if ((rc = run_diamond_pairs(g, &cnt, &t))) return rc;
     *method = JGPM_METHOD_EDGE_TRIANGLE;
   } else if (id >= kIC4 && id <= kIStar3 && !force_enum) {
     uint64_t v[6];

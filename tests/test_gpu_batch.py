@@ -68,7 +68,7 @@ def test_each_job_same_alone_and_in_mix(gpu, mixed):
 
 
 @pytest.mark.parametrize("min_group,split,rpt,isect",
-                         list(itertools.product([4, 8, 32], [8, 32], [8, 256], [0, 1])))
+                         list(itertools.product([4, 8, 32], [32, 128], [8, 256], [0, 1])))
 def test_every_tuning_gives_the_same_counts(gpu, mixed, min_group, split, rpt, isect):
     specs, gs, want = mixed
     jobs = [(g, p) for g in gs[:6] for p in PATTERNS + ["6-clique"]]
@@ -108,3 +108,22 @@ def test_plain_tiers_any_split(gpu, mixed, min_group, split):
             assert g.count(p) == want[(len(gs) - 1, p)]
     finally:
         g.set_tuning(gpu.Tuning(4, 128, 0, 0))
+
+
+def test_batch_large_roots_complete_graph(gpu, mixed):
+    """K_1101 (out-degrees up to 1100, so every root tier including the edge-rooted one)
+    batched with the small graphs: closed-form counts."""
+    from math import comb
+    specs, gs, want = mixed
+    n = 1101
+    iu = np.triu_indices(n, 1)
+    with gpu.Graph.from_edges(iu[0].astype(np.int32), iu[1].astype(np.int32), n) as k:
+        closed = {"triangle": comb(n, 3), "4-clique": comb(n, 4),
+                  "diamond": comb(n, 2) * comb(n - 2, 2), "4-cycle": 3 * comb(n, 4)}
+        jobs = [(k, p) for p in closed] + [(g, p) for g in gs[:4] for p in PATTERNS]
+        counts, _ = gpu.batch_count(jobs)
+        for (g, p), c in zip(jobs, counts):
+            if g is k:
+                assert c == closed[p], p
+            else:
+                assert c == want[(gs.index(g), p)], (gs.index(g), p)

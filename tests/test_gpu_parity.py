@@ -124,6 +124,48 @@ def test_edge_induced_closed_forms(gpu, graphs, name):
     assert g.count("4-cycle") == N["c4"]
 
 
+def complete_graph(J, n):
+    iu = np.triu_indices(n, 1)
+    return J.Graph.from_edges(iu[0].astype(np.int32), iu[1].astype(np.int32), n)
+
+
+def test_large_roots_complete_graph(gpu):
+    """K_1101: every degree ties, so the DAG orders by id and roots 0..75 have out-degree
+    above 1024 (the edge-rooted list tier); the other roots fill every bitmap tier.  All
+    counts have closed forms."""
+    from math import comb
+    n = 1101
+    with complete_graph(gpu, n) as g:
+        assert g.count("triangle") == comb(n, 3)
+        assert g.info()["max_out_degree"] == n - 1
+        assert g.count("k-clique:3") == comb(n, 3)
+        assert g.count("4-clique") == comb(n, 4)
+        assert g.count("diamond") == comb(n, 2) * comb(n - 2, 2)
+        assert g.count("4-cycle") == 3 * comb(n, 4)
+        assert g.count("tailed-triangle") == n * comb(n - 1, 2) * (n - 3)
+        assert g.count("3-star") == n * comb(n - 1, 3)
+        assert g.count("4-path") == 12 * comb(n, 4)
+        assert g.census4() == [0, 0, 0, 0, 0, comb(n, 4)]
+
+
+def test_large_roots_against_oracle(gpu):
+    """A K_1040 planted on the first vertices of an R-MAT graph: large roots next to small
+    ones, checked against the oracle."""
+    base = G.rmat_csr(("plant", 3000, 8, 0.57, 0.19, 0.19, 7))
+    src = np.repeat(np.arange(base.n, dtype=np.int64), np.diff(base.rowptr)).astype(np.int32)
+    iu = np.triu_indices(1040, 1)
+    s = np.concatenate([src, iu[0].astype(np.int32)])
+    d = np.concatenate([base.col.astype(np.int32), iu[1].astype(np.int32)])
+    with gpu.Graph.from_edges(s, d, base.n) as g:
+        rowptr, col = g.csr()
+        sym = O.Csr(len(rowptr) - 1, rowptr, col)
+        dag = O.orient(sym)
+        assert g.count("triangle") == O.count("P0", dag)[0]
+        assert g.info()["max_out_degree"] > 1024
+        # edge-triangle diamond count against the literal P2 plan (no large-root tiers)
+        assert g.count("diamond") == g.count("P2", flags=gpu.COUNT_FORCE_PLAN)
+
+
 @pytest.mark.parametrize("pattern", ["triangle", "4-clique", "5-clique", "P1", "P2", "P7"])
 def test_rounds_do_not_change_counts(gpu, graphs, pattern):
     g = graphs["rmat-n4096-ef8-s5"]
