@@ -54,7 +54,8 @@ struct BatchArgs {
   int c4_ctas;           // CTAs [0, c4_ctas) own a dense counter array and drain the apex queue
   unsigned long long* counts;
   unsigned long long* cursor;  // [0] main queue, [1] large-apex queue
-  int32_t* c4_counters;  // per owner CTA: c4_stride ints, zero between apexes
+  int32_t* c4_counters;  // per owner CTA: c4_stride counters, zero between apexes
+  vid_t* c4_touched;      // per owner CTA: c4_stride touched ids
   int64_t c4_stride;
   int32_t* list_scratch;  // per warp: kLevels lists of list_cap ints
   int64_t list_cap;
@@ -237,11 +238,12 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
   __shared__ uint32_t rows[256];
   __shared__ int degs[256];
   __shared__ unsigned long long s_task;
-  __shared__ int s_cut;
+  __shared__ int s_cut, s_nt;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const bool c4_owner = a.c4_counters && (int)blockIdx.x < a.c4_ctas;
   int32_t* c4 = c4_owner ? a.c4_counters + (int64_t)blockIdx.x * a.c4_stride : nullptr;
+  vid_t* c4t = c4_owner ? a.c4_touched + (int64_t)blockIdx.x * a.c4_stride : nullptr;
   bool c4_done = !c4_owner;
   int smem_kind = -1;  // which layout the dynamic shared memory holds (hash tables persist)
   for (;;) {
@@ -290,7 +292,9 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
         }
         for (int64_t q = t.b; q < t.e; ++q) c += c4_mid_apex(j.rrow, j.rcol, j.mid[q], cta_hash);
         break;
-      case kTaskC4Large: c = c4_large_apex(j.rrow, j.rcol, j.apexes[t.b], c4, &s_cut); break;
+      case kTaskC4Large:
+        c = c4_large_apex(j.rrow, j.rcol, j.apexes[t.b], c4, c4t, &s_cut, &s_nt);
+        break;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
     if (lane == 0 && c) atomicAdd(&a.counts[t.job], c);
@@ -310,11 +314,11 @@ void add_range_tasks(std::vector<Task>& out, int job, int kind, int64_t b, int64
   for (int64_t x = b; x < e; x += chunk) out.push_back(Task{job, kind, x, std::min(e, x + chunk)});
 }
 
-// First index of the root tiers whose out-degree is <= x, x in {32, 64, 128, 512} (tiers
-// sorted by descending out-degree).
+// First index of the root tiers whose out-degree is <= x, x in {32, 64, 128, 256, 512}
+// (tiers sorted by descending out-degree).
 int64_t tier_begin(const RootTiers& t, int x) {
   return x <= 32 ? t.le_begin[0] : x <= 64 ? t.le_begin[1] : x <= 128 ? t.le_begin[2]
-                                                                      : t.le_begin[3];
+         : x <= 256 ? t.le_begin[3] : t.le_begin[4];
 }
 
 struct BuildOut {
@@ -447,7 +451,9 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
       JGPM_CUDA_TRY(cudaMemsetAsync(c.c4.p, 0, c.c4.bytes, s));
       c.c4_zeroed = c.c4.bytes;
     }
+    if ((rc = c.c4t.reserve(need))) return rc;
     a.c4_counters = (int32_t*)c.c4.p;
+    a.c4_touched = (vid_t*)c.c4t.p;
     a.c4_stride = o.c4max;
   }
   if (o.any_large) {

@@ -77,7 +77,7 @@ struct DevArena {
 // scratch).  One per server slot or per synchronous caller.
 struct BatchCtx {
   int device = 0;
-  DevArena jobs, tasks, counts, cursor, c4, lists, tri;
+  DevArena jobs, tasks, counts, cursor, c4, c4t, lists, tri;
   std::vector<JobDesc> h_jobs;
   std::vector<Task> h_tasks;
   int64_t n_c4 = 0;
@@ -85,7 +85,7 @@ struct BatchCtx {
   size_t c4_zeroed = 0;
   size_t c4_cap_bytes = (size_t)4 << 30;  // memory cap of the 4-cycle counter arrays
   ~BatchCtx() {
-    for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &lists, &tri})
+    for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &c4t, &lists, &tri})
       if (d->p) cudaFree(d->p);
   }
 };

@@ -9,7 +9,8 @@
 //   small  (<= kC4SmallBound)  one warp per apex, counts in a shared-memory hash table;
 //   mid    (<= kC4MidBound)    one CTA per apex, counts in a CTA-wide shared-memory table;
 //   large                      one CTA per apex, counts in a dense per-CTA array in global
-//                              memory, heaviest apexes first.
+//                              memory with a list of the touched vertices, heaviest apexes
+//                              first.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -96,9 +97,10 @@ __global__ void __launch_bounds__(256) k_c4_large(const eid_t* rp, const vid_t* 
                                                   const vid_t* list, int64_t nlist,
                                                   unsigned long long* cursor, int32_t* counters,
                                                   DevControl* ctl) {
-  int32_t* dense = counters + (int64_t)blockIdx.x * n;
+  int32_t* dense = counters + (int64_t)blockIdx.x * 2 * n;  // n counters, then n touched ids
+  vid_t* touched = dense + n;
   __shared__ unsigned long long s_q;
-  __shared__ int s_cut;
+  __shared__ int s_cut, s_nt;
   const int tid = threadIdx.x, lane = tid & 31;
   acc_t sum = 0;
   for (;;) {
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(256) k_c4_large(const eid_t* rp, const vid_t* 
     const int64_t q = (int64_t)s_q;
     __syncthreads();
     if (q >= nlist) break;
-    sum += c4_large_apex(rp, col, list[q], dense, &s_cut);
+    sum += c4_large_apex(rp, col, list[q], dense, touched, &s_cut, &s_nt);
   }
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
@@ -204,9 +206,11 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
   const int32_t n = g->n;
   const int sms = device_sm_count(g->device);
   const int64_t nsmall = g->c4_nsmall, nmid = g->c4_nmid, nlarge = g->c4_nlarge;
-  // dense counters for the large apexes: one array of n ints per CTA, within an 8 GiB cap
-  const int64_t per_cta = (int64_t)n * 4;
-  int64_t ctas = std::min<int64_t>((int64_t)sms * 2, ((int64_t)8 << 30) / std::max<int64_t>(1, per_cta));
+  // dense counters and touched lists for the large apexes: 2n ints per CTA, within a 12 GiB
+  // cap
+  const int64_t per_cta = (int64_t)n * 8;
+  int64_t ctas = std::min<int64_t>((int64_t)sms * 2,
+                                   ((int64_t)12 << 30) / std::max<int64_t>(1, per_cta));
   ctas = std::max<int64_t>(1, std::min<int64_t>(ctas, nlarge));
   if (nlarge > 0 && (rc = ensure_scratch(g, (size_t)(ctas * per_cta)))) return rc;
   cudaEvent_t e0, e1;
@@ -238,8 +242,8 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
   }
   if (nlarge > 0) {
     JGPM_CUDA_TRY(cudaMemsetAsync(g->d_scratch, 0, (size_t)(ctas * per_cta), s));
-    k_c4_large<<<(int)ctas, 256, 0, s>>>(g->d_rank_rowptr, g->d_rank_col, n, g->d_c4_large,
-                                         nlarge, &g->d_ctl->counter[1],
+    k_c4_large<<<(int)ctas, 256, 0, s>>>(g->d_rank_rowptr, g->d_rank_col, n,
+                                         g->d_c4_large, nlarge, &g->d_ctl->counter[1],
                                          (int32_t*)g->d_scratch, g->d_ctl);
     g->launches += 1;
   }

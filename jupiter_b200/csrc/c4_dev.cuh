@@ -202,26 +202,34 @@ __device__ __forceinline__ acc_t c4_mid_apex(const eid_t* rp, const vid_t* col, 
   return sum;
 }
 
-// One large apex v on the whole CTA: pass 0 counts the wedges per v3 in the dense array
-// (zero on entry), pass 1 reads and clears them.  Every thread calls it; *s_cut is a shared
-// int.  Returns this thread's share of sum C(c, 2).
+// One large apex v on the whole CTA.  Pass 0 adds every wedge to the dense array (zero on
+// entry) and appends each vertex it counts for the first time to the CTA's touched list;
+// pass 1 reads and clears only the touched counters (distinct vertices, not wedges).  Every
+// thread calls it; s_cut and s_nt are shared ints.  Returns this thread's share of
+// sum C(c, 2).
 __device__ __forceinline__ acc_t c4_large_apex(const eid_t* rp, const vid_t* col, vid_t v,
-                                               int32_t* dense, int* s_cut) {
+                                               int32_t* dense, vid_t* touched, int* s_cut,
+                                               int* s_nt) {
   const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5;
   const eid_t b = rp[v];
   const int d = (int)(rp[v + 1] - b);
-  if (tid == 0) *s_cut = c4_lower_bound(col + b, d, v);
+  if (tid == 0) {
+    *s_cut = c4_lower_bound(col + b, d, v);
+    *s_nt = 0;
+  }
   __syncthreads();
   const int cut = *s_cut;
-  acc_t sum = 0;
-  for (int c0 = warp * 32; c0 < cut; c0 += nw * 32)
-    c4_wedge_chunk(rp, col, v, b, cut, c0, [&](vid_t v3) { atomicAdd(&dense[v3], 1); });
-  __syncthreads();
   for (int c0 = warp * 32; c0 < cut; c0 += nw * 32)
     c4_wedge_chunk(rp, col, v, b, cut, c0, [&](vid_t v3) {
-      const int c = atomicExch(&dense[v3], 0);
-      sum += (acc_t)c * (acc_t)(c - 1) / 2;
+      if (atomicAdd(&dense[v3], 1) == 0) touched[atomicAdd(s_nt, 1)] = v3;
     });
+  __syncthreads();
+  const int nt = *s_nt;
+  acc_t sum = 0;
+  for (int i = tid; i < nt; i += blockDim.x) {
+    const acc_t c = (acc_t)atomicExch(&dense[touched[i]], 0);
+    sum += c * (c - 1) / 2;
+  }
   __syncthreads();
   return sum;
 }

@@ -18,8 +18,12 @@
 //   d <= 4, 8, 16, 32   groups of G = 4, 8, 16, 32 lanes, one root per group; rows are single
 //                       words; L and the row offsets live in registers, searched with
 //                       width-G __shfl_sync;
-//   32 < d <= 1024      one CTA per root; rows of ceil(d/32) words in shared memory; the
-//                       count phase keeps each mask distributed one word per lane;
+//   32 < d <= 128       one warp per root (up to the split degree), rows in the warp's
+//                       slice of shared memory;
+//   split < d <= 1024   one CTA per root; rows of ceil(d/32) words in shared memory, sized
+//                       per degree band (<= 256, <= 512, <= 1024) so that the low bands keep
+//                       many CTAs per SM; masks of up to 8 / 16 words are counted from
+//                       registers, wider ones distributed one word per lane;
 //   d > 1024            edge-rooted fallback: one warp per arc (u, v_i) with the candidate
 //                       lists in per-warp global scratch (the reference's scheme).
 // Work is handed out by global atomic cursors (work stealing); roots are sorted by
@@ -106,7 +110,7 @@ __global__ void __launch_bounds__(256) k_clique_warp(CliqueArgs a) {
 }
 
 // ------------------------------------------------------------------ mid tier (d <= 1024)
-template <int K, bool STATS, bool ETRI = false, bool PAIRS = false>
+template <int K, bool STATS, bool ETRI = false, bool PAIRS = false, int ROWW = kCtaRowWords>
 __global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int W) {
   extern __shared__ __align__(16) unsigned char smem[];
   const MidSmem sm = MidSmem::carve(smem, dmax, W);
@@ -120,7 +124,7 @@ __global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int 
     const int64_t idx = (int64_t)s_idx + a.begin;
     __syncthreads();
     if (idx >= a.end) break;
-    cnt += cta_root<K, STATS, ETRI, PAIRS>(a.rowptr, a.col, a.roots[idx], sm, a.tri, elems);
+    cnt += cta_root<K, STATS, ETRI, PAIRS, ROWW>(a.rowptr, a.col, a.roots[idx], sm, a.tri, elems);
   }
   for (int o = 16; o > 0; o >>= 1) {
     cnt += __shfl_xor_sync(kFull, cnt, o);
@@ -255,14 +259,35 @@ struct TierRange {
   bool empty() const { return e <= b; }
 };
 
-// Launch plan of one count: the root ranges of each tier.
+// Launch plan of one count: the root ranges of each tier.  mid[0..2] are the CTA-root bands
+// of out-degree (512, 1024], (256, 512] and (split, 256].
 struct TierPlan {
-  TierRange large, mid, warp, g32, g16, g8, g4;
+  TierRange large, mid[3], warp, g32, g16, g8, g4;
 };
+
+// One CTA-root band: bitmap layout for out-degree <= dmax, masks of up to ROWW words counted
+// from registers.
+template <int K, bool STATS, bool ETRI, bool PAIRS, int ROWW>
+void launch_mid_band(CliqueArgs a, const TierRange& r, int cursor, int dmax, int sms,
+                     cudaStream_t s) {
+  a.begin = r.b;
+  a.end = r.e;
+  a.cursor = cursor;
+  const int W = (dmax + 31) / 32;
+  const size_t sm = MidLayout{dmax, W}.bytes();
+  auto kern = k_clique_mid<K, STATS, ETRI, PAIRS, ROWW>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, sm);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t roots = r.e - r.b;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, roots));
+  kern<<<grid, 256, sm, s>>>(a, dmax, W);
+}
 
 template <int K, bool STATS, bool ETRI, bool PAIRS = false>
 int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream_t s,
-                  int mid_dmax) {
+                  int max_out) {
   CliqueArgs a = base;
   int n = 0;
   if (!p.large.empty()) {
@@ -272,19 +297,17 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     k_clique_large<K, STATS, ETRI, PAIRS><<<sms * 2, 256, 0, s>>>(a);
     ++n;
   }
-  if (!p.mid.empty()) {
-    a.begin = p.mid.b;
-    a.end = p.mid.e;
-    a.cursor = 1;
-    const int W = (mid_dmax + 31) / 32;
-    const size_t sm = MidLayout{mid_dmax, W}.bytes();
-    cudaFuncSetAttribute(k_clique_mid<K, STATS, ETRI, PAIRS>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clique_mid<K, STATS, ETRI, PAIRS>, 256,
-                                                  sm);
-    if (per_sm < 1) per_sm = 1;
-    k_clique_mid<K, STATS, ETRI, PAIRS><<<sms * per_sm, 256, sm, s>>>(a, mid_dmax, W);
+  if (!p.mid[0].empty()) {
+    launch_mid_band<K, STATS, ETRI, PAIRS, 0>(a, p.mid[0], 1, std::min(max_out, kMidMaxDeg),
+                                              sms, s);
+    ++n;
+  }
+  if (!p.mid[1].empty()) {
+    launch_mid_band<K, STATS, ETRI, PAIRS, 16>(a, p.mid[1], 0, std::min(max_out, 512), sms, s);
+    ++n;
+  }
+  if (!p.mid[2].empty()) {
+    launch_mid_band<K, STATS, ETRI, PAIRS, 8>(a, p.mid[2], 8, std::min(max_out, 256), sms, s);
     ++n;
   }
   if (!p.warp.empty()) {
@@ -334,7 +357,12 @@ static TierPlan make_plan(const RootTiers& t, int k, int64_t root_begin, int64_t
   // 32 < d <= split (split in {32, 64, 128}): warp per root; above: CTA per root
   const int64_t wb = std::max(t.large_end, split >= 128 ? t.le_begin[2]
                                            : split >= 64 ? t.le_begin[1] : t.le_begin[0]);
-  p.mid = cut(t.large_end, wb);
+  // CTA bands (tiers are sorted by descending out-degree, and wb >= b256 >= b512)
+  const int64_t b512 = std::max(t.large_end, t.le_begin[4]);
+  const int64_t b256 = std::max(b512, t.le_begin[3]);
+  p.mid[0] = cut(t.large_end, b512);
+  p.mid[1] = cut(b512, b256);
+  p.mid[2] = cut(b256, wb);
   p.warp = cut(wb, t.mid_end);
   // small tier [mid_end, small_end): d in (16,32] -> G32, (8,16] -> G16, (4,8] -> G8, <=4 -> G4
   const int64_t b16 = min_group <= 16 ? t.deg_begin[16] : t.small_end;
@@ -375,7 +403,7 @@ int launch_clique_ex(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64
     a.scratch = (int32_t*)g->d_scratch;
     a.scratch_per_warp = per_warp;
   }
-  const int mid_dmax = std::max(33, std::min(g->max_out_degree, kMidMaxDeg));
+  const int mid_dmax = std::max(33, g->max_out_degree);
   int n = 0;
   if (tri) {
     n = pairs ? launch_plan_k<3, false, true, true>(a, p, sms, s, mid_dmax)

@@ -25,6 +25,22 @@ __device__ __forceinline__ acc_t pair_gain(unsigned o, unsigned k) {
 
 constexpr int kRangeCut = 32;  // restrict a row to [L0, Ld-1] when longer than this
 
+// Largest power of two <= n (0 for n <= 0).
+__device__ __forceinline__ int top_pow2(int n) { return n > 0 ? 1 << (31 - __clz(n)) : 0; }
+
+// Two independent searches in the same sorted shared-memory array a[0..n) in lockstep:
+// p0 = #{a[j] < x0}, p1 = #{a[j] < x1}.  Binary lifting with a fixed trip count (top =
+// top_pow2(n)), so the two dependent load chains overlap.
+__device__ __forceinline__ void count_below2(const int* a, int n, int top, int x0, int x1,
+                                             int& p0, int& p1) {
+  p0 = 0;
+  p1 = 0;
+  for (int step = top; step > 0; step >>= 1) {
+    if (p0 + step <= n && a[p0 + step - 1] < x0) p0 += step;
+    if (p1 + step <= n && a[p1 + step - 1] < x1) p1 += step;
+  }
+}
+
 // ---------------------------------------------------------------- single-word rows
 template <int D, bool STATS>
 struct SmallCount {
@@ -294,29 +310,29 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
   }
   const int T = ws.off[d];
   acc_t pairs = 0;
-  for (int t = lane; t < T; t += 32) {
-    int lo = 0, hi = d - 1;  // row i: last i with off[i] <= t
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (ws.off[mid] <= t) lo = mid;
-      else hi = mid - 1;
-    }
-    const int i = lo;
-    const vid_t x = __ldg(col + ws.rs[i] + (t - ws.off[i]));
-    int p0 = 0, p1 = d;
-    while (p0 < p1) {
-      const int mid = (p0 + p1) >> 1;
-      if (ws.L[mid] < x) p0 = mid + 1;
-      else p1 = mid;
-    }
-    if (p0 < d && ws.L[p0] == x) {
-      atomicOr(&ws.R[i * w_d + (p0 >> 5)], 1u << (p0 & 31));
+  const int topL = top_pow2(d), topO = top_pow2(d - 1);
+  auto hit = [&](int i, int p, vid_t x, eid_t e) {
+    if (p < d && ws.L[p] == x) {
+      atomicOr(&ws.R[i * w_d + (p >> 5)], 1u << (p & 31));
       if (ETRI) {
-        const unsigned o = atomicAdd(tri + ws.rs[i] + (t - ws.off[i]), 1u);
+        const unsigned o = atomicAdd(tri + e, 1u);
         if (PAIRS) pairs += (acc_t)o;
-        atomicAdd(&ws.colcnt[p0], 1);
+        atomicAdd(&ws.colcnt[p], 1);
       }
     }
+  };
+  // two scanned elements per lane and iteration; row i of element t = last i with off[i] <= t
+  for (int t0 = lane; t0 < T; t0 += 64) {
+    const bool two = t0 + 32 < T;
+    const int t1 = two ? t0 + 32 : t0;
+    int i0, i1;
+    count_below2(ws.off + 1, d - 1, topO, t0 + 1, t1 + 1, i0, i1);
+    const eid_t e0 = ws.rs[i0] + (t0 - ws.off[i0]), e1 = ws.rs[i1] + (t1 - ws.off[i1]);
+    const vid_t x0 = __ldg(col + e0), x1 = __ldg(col + e1);
+    int p0, p1;
+    count_below2(ws.L, d, topL, x0, x1, p0, p1);
+    hit(i0, p0, x0, e0);
+    if (two) hit(i1, p1, x1, e1);
   }
   __syncwarp();
   acc_t cnt = 0;
@@ -439,29 +455,30 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
   }
   const int T = off[d];
   acc_t pairs = 0;
-  for (int t = tid; t < T; t += nthreads) {
-    int lo = 0, hi = d - 1;  // row i: last i with off[i] <= t
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (off[mid] <= t) lo = mid;
-      else hi = mid - 1;
-    }
-    const int i = lo;
-    const vid_t x = __ldg(col + rs[i] + (t - off[i]));
-    int p0 = 0, p1 = d;
-    while (p0 < p1) {
-      const int mid = (p0 + p1) >> 1;
-      if (L[mid] < x) p0 = mid + 1;
-      else p1 = mid;
-    }
-    if (p0 < d && L[p0] == x) {
-      atomicOr(&R[(size_t)i * w_d + (p0 >> 5)], 1u << (p0 & 31));
+  const int topL = top_pow2(d), topO = top_pow2(d - 1);
+  auto hit = [&](int i, int p, vid_t x, eid_t e) {
+    if (p < d && L[p] == x) {
+      atomicOr(&R[(size_t)i * w_d + (p >> 5)], 1u << (p & 31));
       if (ETRI) {
-        const unsigned o = atomicAdd(tri + rs[i] + (t - off[i]), 1u);
+        const unsigned o = atomicAdd(tri + e, 1u);
         if (PAIRS) pairs += (acc_t)o;
-        atomicAdd(&deg[p0], 1);
+        atomicAdd(&deg[p], 1);
       }
     }
+  };
+  // two scanned elements per thread and iteration; row i of element t = last i with
+  // off[i] <= t
+  for (int t0 = tid; t0 < T; t0 += 2 * nthreads) {
+    const bool two = t0 + nthreads < T;
+    const int t1 = two ? t0 + nthreads : t0;
+    int i0, i1;
+    count_below2(off + 1, d - 1, topO, t0 + 1, t1 + 1, i0, i1);
+    const eid_t e0 = rs[i0] + (t0 - off[i0]), e1 = rs[i1] + (t1 - off[i1]);
+    const vid_t x0 = __ldg(col + e0), x1 = __ldg(col + e1);
+    int p0, p1;
+    count_below2(L, d, topL, x0, x1, p0, p1);
+    hit(i0, p0, x0, e0);
+    if (two) hit(i1, p1, x1, e1);
   }
   __syncthreads();
   if (ETRI) {  // the root's own arcs: popc(R_i) + (rows with bit i) triangles each

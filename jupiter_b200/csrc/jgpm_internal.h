@@ -34,7 +34,8 @@ struct RootTiers {
   vid_t* d_roots = nullptr;
   int64_t large_end = 0, mid_end = 0, small_end = 0;
   int64_t deg_begin[34] = {0};
-  int64_t le_begin[4] = {0, 0, 0, 0};  // first index with out-degree <= 32, 64, 128, 512
+  // first index with out-degree <= 32, 64, 128, 256, 512
+  int64_t le_begin[5] = {0, 0, 0, 0, 0};
   int min_deg = -1;  // smallest out-degree kept
 };
 
@@ -42,12 +43,12 @@ struct jgpm_graph_impl;
 
 // Per-launch device control block: work counters, results and the error word.
 struct DevControl {
-  unsigned long long counter[8];  // work-stealing cursors
+  unsigned long long counter[12]; // work-stealing cursors
   unsigned long long count[4];    // pattern results
   unsigned long long elements[4]; // set-op elements (stats launches)
   int error;                      // JGPM_E* raised inside a kernel (0 = none)
   int error_info;
-  int pad[14];
+  int pad[6];
 };
 
 std::string cuda_error_string(cudaError_t e);
