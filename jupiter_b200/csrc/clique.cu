@@ -44,6 +44,8 @@ struct CliqueArgs {
   DevControl* ctl;
   int32_t* scratch;     // large tier: per-warp lists
   int64_t scratch_per_warp;
+  uint32_t* rows;       // CTA tiers with rows in global memory: dmax * W words per CTA
+  int large_chunks;     // list tier: tasks per root (chunks of 32 arcs of the widest root)
   int cursor;           // which ctl->counter this launch steals from
   uint32_t* tri;        // edge-triangle mode: triangles per DAG arc (K == 3 only)
 };
@@ -109,11 +111,15 @@ __global__ void __launch_bounds__(256) k_clique_warp(CliqueArgs a) {
   }
 }
 
-// ------------------------------------------------------------------ mid tier (d <= 1024)
-template <int K, bool STATS, bool ETRI = false, bool PAIRS = false, int ROWW = kCtaRowWords>
+// --------------------------------------------------- CTA tiers (32 < d <= kWideMaxDeg)
+// GR: the bitmap rows live in global scratch (a.rows, dmax * W words per CTA, L2-resident)
+// and the shared memory holds only the root's list and row offsets.
+template <int K, bool STATS, bool ETRI = false, bool PAIRS = false, int ROWW = kCtaRowWords,
+          int WPL = 1, bool GR = false>
 __global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int W) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const MidSmem sm = MidSmem::carve(smem, dmax, W);
+  const MidSmem sm = MidSmem::carve(smem, dmax, W,
+                                    GR ? a.rows + (size_t)blockIdx.x * dmax * W : nullptr);
   __shared__ unsigned long long s_idx;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -124,7 +130,8 @@ __global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int 
     const int64_t idx = (int64_t)s_idx + a.begin;
     __syncthreads();
     if (idx >= a.end) break;
-    cnt += cta_root<K, STATS, ETRI, PAIRS, ROWW>(a.rowptr, a.col, a.roots[idx], sm, a.tri, elems);
+    cnt += cta_root<K, STATS, ETRI, PAIRS, ROWW, WPL, GR>(a.rowptr, a.col, a.roots[idx], sm,
+                                                          a.tri, elems);
   }
   for (int o = 16; o > 0; o >>= 1) {
     cnt += __shfl_xor_sync(kFull, cnt, o);
@@ -176,53 +183,44 @@ __global__ void __launch_bounds__(256) k_clique_large(CliqueArgs a) {
   const int64_t cap = a.scratch_per_warp / kMaxLevels;
   acc_t cnt = 0, elems = 0;
   for (;;) {
-    // task t = arc t of the concatenated arcs of roots [begin, end) (few large roots, so a
-    // linear walk decodes it)
+    // task t = chunk (t mod large_chunks) of 32 arcs of root begin + t / large_chunks
     unsigned long long t = 0;
     if (lane == 0) t = atomicAdd(&a.ctl->counter[a.cursor], 1ull);
     t = __shfl_sync(kFull, t, 0);
-    unsigned long long rem = t;
-    bool found = false;
-    vid_t u = 0;
-    int i = 0;
-    for (int64_t r = a.begin; r < a.end; ++r) {
-      const vid_t ur = a.roots[r];
-      const unsigned long long dr = (unsigned long long)(a.rowptr[ur + 1] - a.rowptr[ur]);
-      if (rem < dr) {
-        u = ur;
-        i = (int)rem;
-        found = true;
-        break;
-      }
-      rem -= dr;
-    }
-    if (!found) break;
+    const int64_t r = a.begin + (int64_t)(t / (unsigned long long)a.large_chunks);
+    if (r >= a.end) break;
+    const vid_t u = a.roots[r];
     const eid_t bu = a.rowptr[u];
     const int du = (int)(a.rowptr[u + 1] - bu);
-    const vid_t v = __ldg(a.col + bu + i);
-    const eid_t bv = a.rowptr[v];
-    const int dv = (int)(a.rowptr[v + 1] - bv);
-    int32_t* W = buf;
-    const int tw = warp_intersect(a.col + bu, du, a.col + bv, dv, INT32_MAX, W);
-    // tw and the ListClique sums are the same in every lane: lane 0 keeps them
-    if (K == 3) {
-      if (!PAIRS && lane == 0) cnt += (acc_t)tw;
-      if (ETRI && tw > 0) {
-        if (lane == 0) {
-          const unsigned o = atomicAdd(a.tri + bu + i, (unsigned)tw);
-          if (PAIRS) cnt += pair_gain(o, (unsigned)tw);
+    const int i0 = (int)(t % (unsigned long long)a.large_chunks) * 32;
+    for (int i = i0; i < min(du, i0 + 32); ++i) {
+      const vid_t v = __ldg(a.col + bu + i);
+      const eid_t bv = a.rowptr[v];
+      const int dv = (int)(a.rowptr[v + 1] - bv);
+      int32_t* W = buf;
+      const int tw = warp_intersect(a.col + bu, du, a.col + bv, dv, INT32_MAX, W);
+      // tw and the ListClique sums are the same in every lane: lane 0 keeps them
+      if (K == 3) {
+        if (!PAIRS && lane == 0) cnt += (acc_t)tw;
+        if (ETRI && tw > 0) {
+          if (lane == 0) {
+            const unsigned o = atomicAdd(a.tri + bu + i, (unsigned)tw);
+            if (PAIRS) cnt += pair_gain(o, (unsigned)tw);
+          }
+          for (int q = lane; q < tw; q += 32) {
+            const vid_t w = W[q];
+            const unsigned o1 = atomicAdd(a.tri + bu + lower_bound_g(a.col + bu, du, w), 1u);
+            const unsigned o2 = atomicAdd(a.tri + bv + lower_bound_g(a.col + bv, dv, w), 1u);
+            if (PAIRS) cnt += (acc_t)o1 + (acc_t)o2;
+          }
+          __syncwarp();
         }
-        for (int q = lane; q < tw; q += 32) {
-          const vid_t w = W[q];
-          const unsigned o1 = atomicAdd(a.tri + bu + lower_bound_g(a.col + bu, du, w), 1u);
-          const unsigned o2 = atomicAdd(a.tri + bv + lower_bound_g(a.col + bv, dv, w), 1u);
-          if (PAIRS) cnt += (acc_t)o1 + (acc_t)o2;
-        }
-        __syncwarp();
+      } else if (tw > 0) {
+        const acc_t c =
+            ListClique<(K > 3 ? K - 3 : 1), STATS>::run(a, W, tw, buf + cap, cap, elems);
+        if (lane == 0) cnt += c;
       }
-    } else if (tw > 0) {
-      const acc_t c = ListClique<(K > 3 ? K - 3 : 1), STATS>::run(a, W, tw, buf + cap, cap, elems);
-      if (lane == 0) cnt += c;
+      __syncwarp();  // W is rewritten by the next arc
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -259,29 +257,41 @@ struct TierRange {
   bool empty() const { return e <= b; }
 };
 
-// Launch plan of one count: the root ranges of each tier.  mid[0..2] are the CTA-root bands
-// of out-degree (512, 1024], (256, 512] and (split, 256].
+// Launch plan of one count: the root ranges of each tier.  wide holds the CTA roots of
+// out-degree (1024, 4096] (rows in global scratch); mid[0..2] are the CTA-root bands of
+// out-degree (512, 1024], (256, 512] and (split, 256].
 struct TierPlan {
-  TierRange large, mid[3], warp, g32, g16, g8, g4;
+  TierRange large, wide, mid[3], warp, g32, g16, g8, g4;
 };
 
+// CTAs and global row words of a wide/global-row band of out-degree <= dmax: at most
+// kRowsBudget bytes of rows so that they stay in L2.
+constexpr size_t kRowsBudget = (size_t)96 << 20;
+inline int rows_band_grid(int dmax, int sms, int64_t roots) {
+  const size_t per = (size_t)dmax * ((dmax + 31) / 32) * 4;
+  const int64_t by_budget = (int64_t)std::max<size_t>(1, kRowsBudget / per);
+  return (int)std::max<int64_t>(
+      1, std::min<int64_t>(std::min<int64_t>((int64_t)sms * 4, by_budget), roots));
+}
+
 // One CTA-root band: bitmap layout for out-degree <= dmax, masks of up to ROWW words counted
-// from registers.
-template <int K, bool STATS, bool ETRI, bool PAIRS, int ROWW>
+// from registers, wider ones with WPL words per lane; GR puts the rows in global scratch.
+template <int K, bool STATS, bool ETRI, bool PAIRS, int ROWW, int WPL = 1, bool GR = false>
 void launch_mid_band(CliqueArgs a, const TierRange& r, int cursor, int dmax, int sms,
                      cudaStream_t s) {
   a.begin = r.b;
   a.end = r.e;
   a.cursor = cursor;
   const int W = (dmax + 31) / 32;
-  const size_t sm = MidLayout{dmax, W}.bytes();
-  auto kern = k_clique_mid<K, STATS, ETRI, PAIRS, ROWW>;
+  const size_t sm = GR ? MidLayout{dmax, W}.bytes_no_rows() : MidLayout{dmax, W}.bytes();
+  auto kern = k_clique_mid<K, STATS, ETRI, PAIRS, ROWW, WPL, GR>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, sm);
   if (per_sm < 1) per_sm = 1;
   const int64_t roots = r.e - r.b;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, roots));
+  int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, roots));
+  if (GR) grid = std::min(grid, rows_band_grid(dmax, sms, roots));
   kern<<<grid, 256, sm, s>>>(a, dmax, W);
 }
 
@@ -295,6 +305,11 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     a.end = p.large.e;
     a.cursor = 2;
     k_clique_large<K, STATS, ETRI, PAIRS><<<sms * 2, 256, 0, s>>>(a);
+    ++n;
+  }
+  if (!p.wide.empty()) {
+    launch_mid_band<K, STATS, ETRI, PAIRS, 0, 4, true>(a, p.wide, 9,
+                                                       std::min(max_out, kWideMaxDeg), sms, s);
     ++n;
   }
   if (!p.mid[0].empty()) {
@@ -353,7 +368,8 @@ static TierPlan make_plan(const RootTiers& t, int k, int64_t root_begin, int64_t
     return r;
   };
   TierPlan p;
-  p.large = cut(0, t.large_end);
+  p.large = cut(0, t.wide_begin);
+  p.wide = cut(t.wide_begin, t.large_end);
   // 32 < d <= split (split in {32, 64, 128}): warp per root; above: CTA per root
   const int64_t wb = std::max(t.large_end, split >= 128 ? t.le_begin[2]
                                            : split >= 64 ? t.le_begin[1] : t.le_begin[0]);
@@ -395,13 +411,24 @@ int launch_clique_ex(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64
   a.roots = t.d_roots;
   a.ctl = g->d_ctl;
   a.tri = tri;
+  // scratch: [per-warp lists of the list tier][bitmap rows of the wide band]
+  size_t list_bytes = 0, row_bytes = 0;
+  int64_t per_warp = 0;
   if (!p.large.empty()) {
-    const int64_t per_warp = (int64_t)kMaxLevels * (g->max_out_degree + 32);
-    const int64_t warps = (int64_t)sms * 2 * 8;
-    int rc = ensure_scratch(g, (size_t)(per_warp * warps) * sizeof(int32_t));
+    a.large_chunks = (g->max_out_degree + 31) / 32;
+    per_warp = (int64_t)kMaxLevels * (g->max_out_degree + 32);
+    list_bytes = (size_t)(per_warp * (int64_t)sms * 2 * 8) * sizeof(int32_t);
+  }
+  if (!p.wide.empty()) {
+    const int dw = std::min(g->max_out_degree, kWideMaxDeg);
+    row_bytes = (size_t)rows_band_grid(dw, sms, p.wide.e - p.wide.b) * dw * ((dw + 31) / 32) * 4;
+  }
+  if (list_bytes + row_bytes > 0) {
+    int rc = ensure_scratch(g, list_bytes + row_bytes);
     if (rc) return rc;
     a.scratch = (int32_t*)g->d_scratch;
     a.scratch_per_warp = per_warp;
+    a.rows = (uint32_t*)((char*)g->d_scratch + list_bytes);
   }
   const int mid_dmax = std::max(33, g->max_out_degree);
   int n = 0;

@@ -157,38 +157,64 @@ __device__ __forceinline__ acc_t group_root(const eid_t* __restrict__ rowptr,
 }
 
 // ---------------------------------------------------------------- multi-word rows
-template <int D, bool STATS>
+// Row loads: rows in global memory (GR) are built with L2 atomics, so they are read at L2
+// (ld.global.cg), never from a possibly stale L1 line; shared-memory rows are read directly.
+template <bool GR>
+__device__ __forceinline__ uint32_t ld_row(const uint32_t* p) {
+  if (GR) return __ldcg(p);
+  return *p;
+}
+
+// Mask distributed over the warp, WPL words per lane: lane l holds words l + 32 q (q < WPL,
+// word index < W).  Rows are W words long.
+template <int D, int WPL, bool STATS, bool GR = false>
 struct DistCount {
-  // Mask distributed one word per lane (lane w holds word w, w < W).
-  __device__ __forceinline__ static acc_t run(uint32_t mw, const uint32_t* R, int W,
-                                              const int* deg, acc_t& elems) {
+  __device__ __forceinline__ static acc_t run(const uint32_t (&mw)[WPL], const uint32_t* R,
+                                              int W, const int* deg, acc_t& elems) {
     const int lane = threadIdx.x & 31;
     acc_t s = 0;
     int pm = 0;
-    if (STATS) pm = __reduce_add_sync(kFull, (unsigned)__popc(mw));
-    unsigned nz = __ballot_sync(kFull, mw != 0u);
-    while (nz) {
-      const int lw = __ffs(nz) - 1;
-      nz &= nz - 1;
-      uint32_t word = __shfl_sync(kFull, mw, lw);
-      while (word) {
-        const int b = __ffs(word) - 1;
-        word &= word - 1;
-        const int j = lw * 32 + b;
-        if (STATS && lane == 0) elems += (acc_t)pm + (acc_t)deg[j];
-        const uint32_t nxt = lane < W ? (mw & R[(size_t)j * W + lane]) : 0u;
-        s += DistCount<D - 1, STATS>::run(nxt, R, W, deg, elems);
+    if (STATS) {
+      int c = 0;
+#pragma unroll
+      for (int q = 0; q < WPL; ++q) c += __popc(mw[q]);
+      pm = __reduce_add_sync(kFull, (unsigned)c);
+    }
+#pragma unroll
+    for (int q = 0; q < WPL; ++q) {
+      unsigned nz = __ballot_sync(kFull, mw[q] != 0u);
+      while (nz) {
+        const int lw = __ffs(nz) - 1;
+        nz &= nz - 1;
+        uint32_t word = __shfl_sync(kFull, mw[q], lw);
+        while (word) {
+          const int b = __ffs(word) - 1;
+          word &= word - 1;
+          const int j = (q * 32 + lw) * 32 + b;
+          if (STATS && lane == 0) elems += (acc_t)pm + (acc_t)deg[j];
+          const uint32_t* Rj = R + (size_t)j * W;
+          uint32_t nxt[WPL];
+#pragma unroll
+          for (int r = 0; r < WPL; ++r) {
+            const int w = r * 32 + lane;
+            nxt[r] = w < W ? (mw[r] & ld_row<GR>(Rj + w)) : 0u;
+          }
+          s += DistCount<D - 1, WPL, STATS, GR>::run(nxt, R, W, deg, elems);
+        }
       }
     }
     return s;
   }
 };
 
-template <bool STATS>
-struct DistCount<0, STATS> {
-  __device__ __forceinline__ static acc_t run(uint32_t mw, const uint32_t*, int, const int*,
-                                              acc_t&) {
-    return (acc_t)__popc(mw);  // per-lane partial; summed at the end
+template <int WPL, bool STATS, bool GR>
+struct DistCount<0, WPL, STATS, GR> {
+  __device__ __forceinline__ static acc_t run(const uint32_t (&mw)[WPL], const uint32_t*, int,
+                                              const int*, acc_t&) {
+    acc_t s = 0;  // per-lane partial; summed at the end
+#pragma unroll
+    for (int q = 0; q < WPL; ++q) s += (acc_t)__popc(mw[q]);
+    return s;
   }
 };
 
@@ -360,9 +386,10 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
 //   deg[dmax] | R[dmax * W] rows | 8 warp sums
 struct MidLayout {
   int dmax, W;
-  __host__ __device__ size_t bytes() const {
+  __host__ __device__ size_t bytes() const { return bytes_no_rows() + (size_t)dmax * W * 4; }
+  __host__ __device__ size_t bytes_no_rows() const {
     return (size_t)dmax * 4 + (size_t)(dmax + 1) * 4 + (size_t)dmax * 8 + (size_t)dmax * 4 +
-           (size_t)dmax * W * 4 + 64 + 64;
+           64 + 64;
   }
 };
 
@@ -373,15 +400,25 @@ struct MidSmem {
   int* deg;
   uint32_t* R;
   int* wsum;
-  __device__ __forceinline__ static MidSmem carve(unsigned char* smem, int dmax, int W) {
+  // rows = nullptr: the rows follow in shared memory (MidLayout); otherwise they live at
+  // rows (dmax * W words of global scratch for this CTA) and shared memory holds the rest
+  // (MidLayout::bytes_no_rows).
+  __device__ __forceinline__ static MidSmem carve(unsigned char* smem, int dmax, int W,
+                                                  uint32_t* rows = nullptr) {
     MidSmem m;
     m.L = reinterpret_cast<vid_t*>(smem);
     m.off = reinterpret_cast<int*>(m.L + dmax);
     m.rs = reinterpret_cast<eid_t*>(
         (reinterpret_cast<uintptr_t>(m.off + dmax + 1) + 7) & ~uintptr_t(7));
     m.deg = reinterpret_cast<int*>(m.rs + dmax);
-    m.R = reinterpret_cast<uint32_t*>(m.deg + dmax);
-    m.wsum = reinterpret_cast<int*>(m.R + (size_t)dmax * W);
+    uint32_t* after = reinterpret_cast<uint32_t*>(m.deg + dmax);
+    if (rows) {
+      m.R = rows;
+      m.wsum = reinterpret_cast<int*>(after);
+    } else {
+      m.R = after;
+      m.wsum = reinterpret_cast<int*>(m.R + (size_t)dmax * W);
+    }
     return m;
   }
 };
@@ -391,8 +428,10 @@ constexpr int kCtaRowWords = 16;
 
 // One root of out-degree 32 < d <= dmax processed by the whole CTA (blockDim = 256).
 // Every thread calls it; returns this thread's partial count.  Rows of up to ROWW words are
-// counted row-parallel from registers, wider ones (or all, with ROWW = 0) warp-cooperatively.
-template <int K, bool STATS, bool ETRI, bool PAIRS = false, int ROWW = kCtaRowWords>
+// counted row-parallel from registers, wider ones (or all, with ROWW = 0) warp-cooperatively
+// with WPL mask words per lane (rows of up to 32 WPL words).
+template <int K, bool STATS, bool ETRI, bool PAIRS = false, int ROWW = kCtaRowWords,
+          int WPL = 1, bool GR = false>
 __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
                                           const vid_t* __restrict__ col, vid_t u,
                                           const MidSmem& sm, uint32_t* tri, acc_t& elems) {
@@ -484,7 +523,7 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
   if (ETRI) {  // the root's own arcs: popc(R_i) + (rows with bit i) triangles each
     for (int i = tid; i < d; i += nthreads) {
       unsigned tu = (unsigned)deg[i];
-      for (int q = 0; q < w_d; ++q) tu += (unsigned)__popc(R[(size_t)i * w_d + q]);
+      for (int q = 0; q < w_d; ++q) tu += (unsigned)__popc(ld_row<GR>(R + (size_t)i * w_d + q));
       if (tu) {
         const unsigned o = atomicAdd(tri + base + i, tu);
         if (PAIRS) pairs += pair_gain(o, tu);
@@ -496,6 +535,7 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
     return pairs;
   }
   acc_t cnt = 0;
+  static_assert(!GR || ROWW == 0, "rows in global memory are counted warp-cooperatively");
   constexpr int RW = ROWW > 0 ? ROWW : 1;
   if (ROWW > 0 && w_d <= ROWW) {
     // row-parallel: each thread owns rows, masks in registers
@@ -506,10 +546,15 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
       cnt += RowCount<K - 3, RW, STATS>::run(m, R, w_d, deg, elems);
     }
   } else {
-    // very wide rows: the mask is distributed one word per lane
+    // wide rows: the mask is distributed over the lanes, WPL words each
     for (int i = warp; i < d; i += nwarps) {
-      const uint32_t mw = lane < w_d ? R[(size_t)i * w_d + lane] : 0u;
-      cnt += DistCount<K - 3, STATS>::run(mw, R, w_d, deg, elems);
+      uint32_t mw[WPL];
+#pragma unroll
+      for (int q = 0; q < WPL; ++q) {
+        const int w = q * 32 + lane;
+        mw[q] = w < w_d ? ld_row<GR>(R + (size_t)i * w_d + w) : 0u;
+      }
+      cnt += DistCount<K - 3, WPL, STATS, GR>::run(mw, R, w_d, deg, elems);
     }
   }
   __syncthreads();

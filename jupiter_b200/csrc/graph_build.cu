@@ -458,15 +458,17 @@ int ensure_tiers(jgpm_graph* g, int min_deg) {
   JGPM_CUDA_TRY(cudaMemcpyAsync(g->tiers.d_roots, v1.p, (size_t)n * sizeof(int32_t),
                                 cudaMemcpyDeviceToDevice, s));
   JGPM_CUDA_TRY(cudaStreamSynchronize(s));
-  int64_t n_large = 0, n_mid = 0, n_small = 0;
+  int64_t n_large = 0, n_mid = 0, n_small = 0, n_wide_plus = 0;
   for (int32_t i = 0; i < n; ++i) {
     uint32_t d = hk[i];
     if (d == 0) break;
+    if (d > (uint32_t)kWideMaxDeg) ++n_wide_plus;
     if (d > (uint32_t)kMidMaxDeg) ++n_large;
     else if (d > 32u) ++n_mid;
     else ++n_small;
   }
   g->tiers.large_end = n_large;
+  g->tiers.wide_begin = n_wide_plus;
   g->tiers.mid_end = n_large + n_mid;
   g->tiers.small_end = n_large + n_mid + n_small;
   // deg_begin[x]: first index with out-degree <= x (keys are sorted descending)

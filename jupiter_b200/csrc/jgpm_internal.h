@@ -27,6 +27,9 @@ struct DevCsr {
 //   mid    [large_end, mid_end)    32 < d <= kMidMaxDeg
 //   small  [mid_end, small_end)    min_deg <= d <= 32
 constexpr int kMidMaxDeg = 1024;
+// Roots of out-degree kMidMaxDeg < d <= kWideMaxDeg still run on local bitmaps, with the
+// bitmap rows in global scratch; larger ones run on edge-rooted lists.
+constexpr int kWideMaxDeg = 4096;
 
 //   deg_begin[x] = first index whose out-degree is <= x (0 <= x <= 33), so the roots with
 //   d >= k-1 are the prefix [0, deg_begin[k-2]).
@@ -36,6 +39,7 @@ struct RootTiers {
   int64_t deg_begin[34] = {0};
   // first index with out-degree <= 32, 64, 128, 256, 512
   int64_t le_begin[5] = {0, 0, 0, 0, 0};
+  int64_t wide_begin = 0;  // first index with out-degree <= kWideMaxDeg
   int min_deg = -1;  // smallest out-degree kept
 };
 

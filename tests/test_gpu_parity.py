@@ -148,6 +148,31 @@ def test_large_roots_complete_graph(gpu):
         assert g.census4() == [0, 0, 0, 0, 0, comb(n, 4)]
 
 
+def test_list_tier_crown(gpu):
+    """Roots of out-degree above 4096 run on edge-rooted lists.  Crown graph: A = 5000
+    vertices in 1250 disjoint K4s, B = 5001 vertices joined to all of A, and a hub h joined
+    to all of A.  Degrees: a 5005, b 5000, h 5000, so h and every b point to all of A
+    (out-degree 5000).  With g = 1250 groups: triangles 4g + 6g + 6g|B|, 4-cliques
+    g + 4g + 4g|B|, 5-cliques g(1 + |B|), diamonds 3 (|A| + |A||B|) + 6g C(|B| + 3, 2)."""
+    from math import comb
+    na, nb, g = 5000, 5001, 1250
+    a = np.arange(na, dtype=np.int64)
+    b = np.arange(na, na + nb, dtype=np.int64)
+    h = na + nb
+    grp = a.reshape(g, 4)
+    iu = np.triu_indices(4, 1)
+    src = [np.repeat(a, nb), np.full(na, h), grp[:, iu[0]].ravel()]
+    dst = [np.tile(b, na), a, grp[:, iu[1]].ravel()]
+    s = np.concatenate(src).astype(np.int32)
+    d = np.concatenate(dst).astype(np.int32)
+    with gpu.Graph.from_edges(s, d, h + 1) as G_:
+        assert G_.count("triangle") == 4 * g + 6 * g + 6 * g * nb
+        assert G_.info()["max_out_degree"] == na
+        assert G_.count("4-clique") == g + 4 * g + 4 * g * nb
+        assert G_.count("5-clique") == g * (1 + nb)
+        assert G_.count("diamond") == 3 * (na + na * nb) + 6 * g * comb(nb + 3, 2)
+
+
 def test_large_roots_against_oracle(gpu):
     """A K_1040 planted on the first vertices of an R-MAT graph: large roots next to small
     ones, checked against the oracle."""
