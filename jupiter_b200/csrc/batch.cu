@@ -12,7 +12,9 @@
 //   WARP_ROOTS  roots with 32 < d <= split, one root per warp (bitmap in the warp's shared
 //               slice);
 //   CTA_ROOT    one root with split < d <= kBatchCtaMaxDeg on the whole CTA;
-//   LARGE_ROOT  one root with d > kBatchCtaMaxDeg, edge-rooted lists in warp scratch;
+//   WIDE_ROOT   one root with kBatchCtaMaxDeg < d <= kBatchWideMaxDeg on the whole CTA, bitmap
+//               rows in per-CTA global scratch (read at L2);
+//   LARGE_ROOT  one root with d > kBatchWideMaxDeg, edge-rooted lists in warp scratch;
 //   C4_SMALL    4-cycle apexes with few wedges, one per warp (shared-memory hash);
 //   C4_MID      4-cycle apexes with up to 2048 wedges, each on the whole CTA (shared hash);
 //   C4_LARGE    one heavy 4-cycle apex on the whole CTA (dense counters in global memory).
@@ -60,6 +62,8 @@ struct BatchArgs {
   int32_t* list_scratch;  // per warp: kLevels lists of list_cap ints
   int64_t list_cap;
   int dmax, W;            // CTA-root bitmap layout
+  uint32_t* rows;         // wide roots: wdmax * wW words of bitmap rows per CTA
+  int wdmax, wW;
   int intersect;          // last clique level of large roots: 0 search from the shorter list,
                           // 1 always from the candidate list
 };
@@ -69,11 +73,12 @@ namespace {
 constexpr int kLevels = 6;
 
 // Shared memory of one CTA of the batched kernel: the largest of the per-kind layouts.
-inline size_t batch_smem_bytes(int dmax, int W) {
+inline size_t batch_smem_bytes(int dmax, int W, int wdmax, int wW) {
   size_t b = 8 * sizeof(WarpSmem);
   b = std::max(b, 8 * sizeof(C4WarpHash));
   b = std::max(b, sizeof(C4CtaHash));
   b = std::max(b, MidLayout{dmax, W}.bytes());
+  if (wdmax > 0) b = std::max(b, MidLayout{wdmax, wW}.bytes_no_rows());
   return b;
 }
 
@@ -177,6 +182,22 @@ __device__ __forceinline__ acc_t task_cta_root(const JobDesc& j, vid_t u, const 
   }
 }
 
+// One wide root (rows in global scratch, masks two words per lane).
+__device__ __forceinline__ acc_t task_wide_root(const JobDesc& j, vid_t u, const MidSmem& sm) {
+  acc_t el = 0;
+  if (j.kind == kJobDiamond)
+    return cta_root<3, false, true, true, 0, 2, true>(j.drow, j.dcol, u, sm, j.tri, el);
+  switch (j.k) {
+    case 3: return cta_root<3, false, false, false, 0, 2, true>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 4: return cta_root<4, false, false, false, 0, 2, true>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 5: return cta_root<5, false, false, false, 0, 2, true>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 6: return cta_root<6, false, false, false, 0, 2, true>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 7: return cta_root<7, false, false, false, 0, 2, true>(j.drow, j.dcol, u, sm, nullptr, el);
+    default:
+      return cta_root<8, false, false, false, 0, 2, true>(j.drow, j.dcol, u, sm, nullptr, el);
+  }
+}
+
 // Warps of the CTA take the arcs (u, v_i) of the large root u: W = N+(u) & N+(v_i) in warp
 // scratch, then the deeper clique levels on lists (or, for diamond jobs, the pair counts of
 // the triangles (u, v_i, w)).  Returns this lane's partial.
@@ -238,7 +259,7 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
   __shared__ uint32_t rows[256];
   __shared__ int degs[256];
   __shared__ unsigned long long s_task;
-  __shared__ int s_cut, s_nt;
+  __shared__ C4LargeSmem s_c4l;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const bool c4_owner = a.c4_counters && (int)blockIdx.x < a.c4_ctas;
@@ -277,6 +298,13 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
         smem_kind = kTaskCtaRoot;
         c = task_cta_root(j, j.roots[t.b], sm);
         break;
+      case kTaskWideRoot: {
+        smem_kind = kTaskWideRoot;
+        const MidSmem wsm = MidSmem::carve(
+            smem, a.wdmax, a.wW, a.rows + (size_t)blockIdx.x * a.wdmax * a.wW);
+        c = task_wide_root(j, j.roots[t.b], wsm);
+        break;
+      }
       case kTaskLargeRoot: c = task_large_root(j, j.roots[t.b], a); break;
       case kTaskC4Small:
         if (smem_kind != kTaskC4Small) {
@@ -293,7 +321,7 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
         for (int64_t q = t.b; q < t.e; ++q) c += c4_mid_apex(j.rrow, j.rcol, j.mid[q], cta_hash);
         break;
       case kTaskC4Large:
-        c = c4_large_apex(j.rrow, j.rcol, j.apexes[t.b], c4, c4t, &s_cut, &s_nt);
+        c = c4_large_apex(j.rrow, j.rcol, j.apexes[t.b], c4, c4t, s_c4l);
         break;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
@@ -323,6 +351,7 @@ int64_t tier_begin(const RootTiers& t, int x) {
 
 struct BuildOut {
   int dmax = 33;          // largest CTA-root out-degree
+  int wdmax = 0;          // largest wide-root out-degree (0: no wide roots)
   int64_t c4max = 0;      // largest vertex count of a job with large 4-cycle apexes
   int max_out = 0;        // largest out-degree among the large roots
   bool any_large = false;
@@ -372,15 +401,21 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
       o->tri_bytes += ((size_t)std::max<int64_t>(1, g->m_dag) * 4 + 255) & ~(size_t)255;
     }
     const int64_t stop = t.deg_begin[jd.k - 2];  // roots with d >= k-1
-    // roots by out-degree: > 512 large | (split, 512] CTA | (32, split] warp | <= 32 groups
+    // roots by out-degree: > 2048 large | (512, 2048] wide | (split, 512] CTA |
+    // (32, split] warp | <= 32 groups
+    const int64_t wide_begin = std::min(stop, t.le_begin[5]);
     const int64_t large_end = std::min(stop, tier_begin(t, kBatchCtaMaxDeg));
     const int64_t cta_end = std::min(stop, std::max(large_end, tier_begin(t, split)));
     const int64_t warp_end = std::min(stop, std::max(cta_end, t.deg_begin[32]));
-    for (int64_t r = 0; r < large_end; ++r) heavy.push_back(Task{job, kTaskLargeRoot, r, r + 1});
-    if (large_end > 0) {
+    for (int64_t r = 0; r < wide_begin; ++r) heavy.push_back(Task{job, kTaskLargeRoot, r, r + 1});
+    if (wide_begin > 0) {
       o->any_large = true;
       o->max_out = std::max(o->max_out, g->max_out_degree);
     }
+    for (int64_t r = wide_begin; r < large_end; ++r)
+      heavy.push_back(Task{job, kTaskWideRoot, r, r + 1});
+    if (large_end > wide_begin)
+      o->wdmax = std::max(o->wdmax, std::min(g->max_out_degree, kBatchWideMaxDeg));
     for (int64_t r = large_end; r < cta_end; ++r) cta.push_back(Task{job, kTaskCtaRoot, r, r + 1});
     if (cta_end > large_end)
       o->dmax = std::max(o->dmax, std::min(g->max_out_degree, kBatchCtaMaxDeg));
@@ -423,7 +458,8 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   if ((rc = build_tasks(in, tu, c, &o))) return rc;
   const int sms = device_sm_count(c.device);
   const int W = (o.dmax + 31) / 32;
-  const size_t smem = batch_smem_bytes(o.dmax, W);
+  const int wW = (o.wdmax + 31) / 32;
+  const size_t smem = batch_smem_bytes(o.dmax, W, o.wdmax, wW);
   cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, 256, smem);
@@ -455,6 +491,12 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     a.c4_counters = (int32_t*)c.c4.p;
     a.c4_touched = (vid_t*)c.c4t.p;
     a.c4_stride = o.c4max;
+  }
+  if (o.wdmax > 0) {
+    if ((rc = c.rows.reserve((size_t)grid * o.wdmax * wW * sizeof(uint32_t)))) return rc;
+    a.rows = (uint32_t*)c.rows.p;
+    a.wdmax = o.wdmax;
+    a.wW = wW;
   }
   if (o.any_large) {
     a.list_cap = o.max_out + 32;

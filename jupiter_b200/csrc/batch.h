@@ -22,15 +22,20 @@ enum TaskKind : int32_t {
   kTaskGroup32 = 3,
   kTaskWarpRoots = 4,  // roots [b, e) of out-degree 32 < d <= split, one per warp
   kTaskCtaRoot = 5,    // root b, split < d <= kBatchCtaMaxDeg, the whole CTA
-  kTaskLargeRoot = 6,  // root b, d > kBatchCtaMaxDeg, warps take its arcs (edge-rooted lists)
+  kTaskLargeRoot = 6,  // root b, d > kBatchWideMaxDeg, warps take its arcs (edge-rooted lists)
   kTaskC4Small = 7,    // small 4-cycle apexes [b, e) of the job's list, one per warp
   kTaskC4Large = 8,    // large 4-cycle apex b of the job's list, the whole CTA
   kTaskC4Mid = 9,      // mid 4-cycle apexes [b, e) of the job's list, one after another per CTA
+  kTaskWideRoot = 10,  // root b, kBatchCtaMaxDeg < d <= kBatchWideMaxDeg, the whole CTA with
+                       // its bitmap rows in global scratch
 };
 
-// Out-degree above which a batched root runs on the edge-rooted list path (the CTA bitmap of
-// a root of out-degree d takes about 20 d + d^2 / 8 bytes of shared memory).
+// Out-degree limits of the batched root tasks: the CTA bitmap of a root of out-degree d takes
+// about 20 d + d^2 / 8 bytes; up to kBatchCtaMaxDeg all of it is in shared memory, up to
+// kBatchWideMaxDeg the d^2 / 8 bytes of rows go to global scratch, above that the root runs on
+// edge-rooted lists.
 constexpr int kBatchCtaMaxDeg = 512;
+constexpr int kBatchWideMaxDeg = 2048;
 
 struct JobDesc {
   const eid_t* drow;    // DAG (cliques, diamond)
@@ -77,7 +82,7 @@ struct DevArena {
 // scratch).  One per server slot or per synchronous caller.
 struct BatchCtx {
   int device = 0;
-  DevArena jobs, tasks, counts, cursor, c4, c4t, lists, tri;
+  DevArena jobs, tasks, counts, cursor, c4, c4t, lists, tri, rows;
   std::vector<JobDesc> h_jobs;
   std::vector<Task> h_tasks;
   int64_t n_c4 = 0;
@@ -85,7 +90,7 @@ struct BatchCtx {
   size_t c4_zeroed = 0;
   size_t c4_cap_bytes = (size_t)4 << 30;  // memory cap of the 4-cycle counter arrays
   ~BatchCtx() {
-    for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &c4t, &lists, &tri})
+    for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &c4t, &lists, &tri, &rows})
       if (d->p) cudaFree(d->p);
   }
 };

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256) k_c4_large(const eid_t* rp, const vid_t* 
   int32_t* dense = counters + (int64_t)blockIdx.x * 2 * n;  // n counters, then n touched ids
   vid_t* touched = dense + n;
   __shared__ unsigned long long s_q;
-  __shared__ int s_cut, s_nt;
+  __shared__ C4LargeSmem sh;
   const int tid = threadIdx.x, lane = tid & 31;
   acc_t sum = 0;
   for (;;) {
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256) k_c4_large(const eid_t* rp, const vid_t* 
     const int64_t q = (int64_t)s_q;
     __syncthreads();
     if (q >= nlist) break;
-    sum += c4_large_apex(rp, col, list[q], dense, touched, &s_cut, &s_nt);
+    sum += c4_large_apex(rp, col, list[q], dense, touched, sh);
   }
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);

@@ -44,6 +44,8 @@ struct C4CtaHash {
   int pad[2];
 };
 
+__device__ __forceinline__ int top_pow2_c4(int n) { return n > 0 ? 1 << (31 - __clz(n)) : 0; }
+
 __device__ __forceinline__ int c4_lower_bound(const vid_t* a, int n, vid_t key) {
   int lo = 0, hi = n;
   while (lo < hi) {
@@ -202,32 +204,88 @@ __device__ __forceinline__ acc_t c4_mid_apex(const eid_t* rp, const vid_t* col, 
   return sum;
 }
 
-// One large apex v on the whole CTA.  Pass 0 adds every wedge to the dense array (zero on
-// entry) and appends each vertex it counts for the first time to the CTA's touched list;
-// pass 1 reads and clears only the touched counters (distinct vertices, not wedges).  Every
-// thread calls it; s_cut and s_nt are shared ints.  Returns this thread's share of
+// Shared memory of the large-apex path (blockDim <= 256).
+struct C4LargeSmem {
+  int cut, nt;
+  int off[257];   // exclusive offsets of the block's x wedge counts, off[256] = total
+  int wsum[8];
+  eid_t bx[256];  // start of prefix(N(x), v) for the block's x
+};
+
+// Binary lifting over a sorted shared-memory array (fixed trip count, top = largest power of
+// two <= n): two independent searches in lockstep, p = #{a[j] < x}.
+__device__ __forceinline__ void c4_count_below2(const int* a, int n, int top, int x0, int x1,
+                                                int& p0, int& p1) {
+  p0 = 0;
+  p1 = 0;
+  for (int step = top; step > 0; step >>= 1) {
+    if (p0 + step <= n && a[p0 + step - 1] < x0) p0 += step;
+    if (p1 + step <= n && a[p1 + step - 1] < x1) p1 += step;
+  }
+}
+
+// One large apex v on the whole CTA.  The lower-ranked neighbours x are taken in blocks of
+// blockDim; each block's wedges (one thread computes |prefix(N(x), v)| per x, a block scan
+// gives the offsets) are spread over all threads, two per thread and iteration, so one hub x
+// does not hold up a single warp.  Pass 0 adds every wedge to the dense array (zero on entry)
+// and appends each vertex counted for the first time to the touched list; pass 1 reads and
+// clears only the touched counters.  Every thread calls it.  Returns this thread's share of
 // sum C(c, 2).
 __device__ __forceinline__ acc_t c4_large_apex(const eid_t* rp, const vid_t* col, vid_t v,
-                                               int32_t* dense, vid_t* touched, int* s_cut,
-                                               int* s_nt) {
-  const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5;
+                                               int32_t* dense, vid_t* touched,
+                                               C4LargeSmem& sh) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nth = blockDim.x, nw = nth >> 5;
   const eid_t b = rp[v];
   const int d = (int)(rp[v + 1] - b);
   if (tid == 0) {
-    *s_cut = c4_lower_bound(col + b, d, v);
-    *s_nt = 0;
+    sh.cut = c4_lower_bound(col + b, d, v);
+    sh.nt = 0;
   }
   __syncthreads();
-  const int cut = *s_cut;
-  for (int c0 = warp * 32; c0 < cut; c0 += nw * 32)
-    c4_wedge_chunk(rp, col, v, b, cut, c0, [&](vid_t v3) {
-      if (atomicAdd(&dense[v3], 1) == 0) touched[atomicAdd(s_nt, 1)] = v3;
-    });
-  __syncthreads();
-  const int nt = *s_nt;
+  const int cut = sh.cut;
+  for (int base = 0; base < cut; base += nth) {
+    const int i = base + tid;
+    int len = 0;
+    eid_t bx = 0;
+    if (i < cut) {
+      const vid_t x = __ldg(col + b + i);
+      bx = rp[x];
+      len = c4_lower_bound(col + bx, (int)(rp[x + 1] - bx), v);
+    }
+    // block exclusive scan of len
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) sh.wsum[warp] = incl;
+    __syncthreads();
+    int wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += sh.wsum[w];
+    sh.off[tid] = wbase + incl - len;
+    sh.bx[tid] = bx;
+    if (tid == nth - 1) sh.off[nth] = wbase + incl;
+    __syncthreads();
+    const int T = sh.off[nth];
+    const int top = top_pow2_c4(nth - 1);
+    for (int t0 = tid; t0 < T; t0 += 2 * nth) {
+      const bool two = t0 + nth < T;
+      const int t1 = two ? t0 + nth : t0;
+      int r0, r1;  // row of element t = last r with off[r] <= t
+      c4_count_below2(sh.off + 1, nth - 1, top, t0 + 1, t1 + 1, r0, r1);
+      const vid_t v30 = __ldg(col + sh.bx[r0] + (t0 - sh.off[r0]));
+      const vid_t v31 = __ldg(col + sh.bx[r1] + (t1 - sh.off[r1]));
+      if (atomicAdd(&dense[v30], 1) == 0) touched[atomicAdd(&sh.nt, 1)] = v30;
+      if (two && atomicAdd(&dense[v31], 1) == 0) touched[atomicAdd(&sh.nt, 1)] = v31;
+    }
+    __syncthreads();
+  }
+  const int nt = sh.nt;
   acc_t sum = 0;
-  for (int i = tid; i < nt; i += blockDim.x) {
-    const acc_t c = (acc_t)atomicExch(&dense[touched[i]], 0);
+  for (int q = tid; q < nt; q += nth) {
+    const acc_t c = (acc_t)atomicExch(&dense[touched[q]], 0);
     sum += c * (c - 1) / 2;
   }
   __syncthreads();

@@ -481,8 +481,8 @@ int ensure_tiers(jgpm_graph* g, int min_deg) {
     }
     g->tiers.deg_begin[x] = lo;
   }
-  const uint32_t le_thr[5] = {32u, 64u, 128u, 256u, 512u};
-  for (int q = 0; q < 5; ++q) {
+  const uint32_t le_thr[6] = {32u, 64u, 128u, 256u, 512u, 2048u};
+  for (int q = 0; q < 6; ++q) {
     int64_t lo = 0, hi = g->tiers.small_end;
     while (lo < hi) {
       const int64_t mid = (lo + hi) >> 1;

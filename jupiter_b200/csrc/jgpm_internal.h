@@ -37,8 +37,8 @@ struct RootTiers {
   vid_t* d_roots = nullptr;
   int64_t large_end = 0, mid_end = 0, small_end = 0;
   int64_t deg_begin[34] = {0};
-  // first index with out-degree <= 32, 64, 128, 256, 512
-  int64_t le_begin[5] = {0, 0, 0, 0, 0};
+  // first index with out-degree <= 32, 64, 128, 256, 512, 2048
+  int64_t le_begin[6] = {0, 0, 0, 0, 0, 0};
   int64_t wide_begin = 0;  // first index with out-degree <= kWideMaxDeg
   int min_deg = -1;  // smallest out-degree kept
 };

@@ -7,7 +7,9 @@
 // arrived while others run overlap on the device.  Admission: a query's graph must be
 // resident (the pool uploads it again, evicting least-recently-used idle graphs, if needed)
 // and the resident graph bytes plus the estimated frontier memory of everything in flight
-// must stay within the budget.  Counts are those of the batched kernel, i.e. exact and
+// must stay within the budget.  A batch's frontier is the sum of its queries' own scratch
+// (diamond per-arc counters) plus the largest shared scratch any of them needs (4-cycle
+// counter arena, edge-rooted list scratch), since the batch shares one context.  Counts are those of the batched kernel, i.e. exact and
 // identical to the plain per-query path.
 #include <cuda_runtime.h>
 
@@ -42,7 +44,9 @@ struct Query {
   int kind = 0, k = 0;
   double t_submit = 0.0, t_done = 0.0;
   uint64_t count = 0;
-  uint64_t frontier = 0;
+  uint64_t frontier = 0;       // plain lane: bytes this query may allocate while it runs
+  uint64_t fr_own = 0;         // batched: scratch of this query alone (adds up in a batch)
+  uint64_t fr_shared = 0;      // batched: shared scratch of the batch this query needs
   int status = 1;  // 1 pending, 0 done, < 0 error
   bool plain = false;   // not batchable: runs through jgpm_count on the plain lane
   int induced = 0;
@@ -65,6 +69,7 @@ struct Slot {
   cudaEvent_t done_ev = nullptr;
   uint64_t* h_counts = nullptr;  // pinned
   std::vector<std::shared_ptr<Query>> queries;
+  uint64_t frontier = 0;  // of the batch in flight
   bool busy = false;
 };
 
@@ -132,23 +137,25 @@ int make_resident(jgpm_server* s, int gid, uint64_t frontier) {
 int launch_batch(jgpm_server* s, Slot& slot) {
   std::vector<std::shared_ptr<Query>> batch;
   std::vector<BatchJobIn> in;
-  uint64_t frontier = 0;
+  uint64_t own = 0, shared = 0;
   for (auto it = s->pending.begin(); it != s->pending.end() && (int)batch.size() < s->cfg.max_batch;) {
     std::shared_ptr<Query> q = *it;
     PoolGraph& pg = s->graphs[q->graph_id];
+    const uint64_t with_q = own + q->fr_own + std::max(shared, q->fr_shared);
     if (!pg.resident) {
-      int rc = make_resident(s, q->graph_id, frontier + q->frontier);
+      int rc = make_resident(s, q->graph_id, with_q);
       if (rc == JGPM_EBUSY) {
         ++it;
         continue;
       }
       if (rc) return rc;
     }
-    if (over_budget(s, frontier + q->frontier) && (!batch.empty() || s->inflight_frontier > 0)) {
+    if (over_budget(s, with_q) && (!batch.empty() || s->inflight_frontier > 0)) {
       ++it;  // wait for in-flight work to release memory
       continue;
     }
-    frontier += q->frontier;
+    own += q->fr_own;
+    shared = std::max(shared, q->fr_shared);
     pg.inflight++;
     pg.last_use = ++s->use_clock;
     in.push_back(BatchJobIn{pg.g, q->kind, q->k});
@@ -167,7 +174,9 @@ int launch_batch(jgpm_server* s, Slot& slot) {
     return rc;
   }
   cudaEventRecord(slot.done_ev, slot.stream);
+  const uint64_t frontier = own + shared;
   s->inflight_frontier += frontier;
+  slot.frontier = frontier;
   s->st.peak_frontier_bytes = std::max<uint64_t>(s->st.peak_frontier_bytes, s->inflight_frontier);
   s->st.batches++;
   slot.queries = std::move(batch);
@@ -183,9 +192,17 @@ void complete_slot(jgpm_server* s, Slot& slot) {
     q.t_done = t;
     q.status = 0;
     s->graphs[q.graph_id].inflight--;
-    s->inflight_frontier -= q.frontier;
     s->st.completed++;
   }
+  // derived structures (DAG, tiers, 4-cycle classes) may have grown the graphs
+  for (auto& qp : slot.queries) {
+    PoolGraph& pg = s->graphs[qp->graph_id];
+    const uint64_t b = graph_device_bytes(pg.g);
+    s->resident_bytes += b - pg.bytes;
+    pg.bytes = b;
+  }
+  s->inflight_frontier -= slot.frontier;
+  slot.frontier = 0;
   slot.queries.clear();
   slot.busy = false;
 }
@@ -263,7 +280,13 @@ void plain_worker(jgpm_server* s) {
     const int rc = jgpm_count_ex(g, q->pattern.c_str(), q->induced, 1, 0u, &cnt, nullptr);
     const std::string err = rc ? std::string(jgpm_last_error()) : std::string();
     lk.lock();
-    s->graphs[q->graph_id].inflight--;
+    {
+      PoolGraph& pg2 = s->graphs[q->graph_id];
+      pg2.inflight--;
+      const uint64_t b = graph_device_bytes(pg2.g);
+      s->resident_bytes += b - pg2.bytes;
+      pg2.bytes = b;
+    }
     s->inflight_frontier -= q->frontier;
     q->count = cnt;
     q->t_done = now_s();
@@ -281,17 +304,29 @@ using namespace jgpm;
 
 namespace {
 
-uint64_t estimate_frontier(const jgpm_server* s, const jgpm_graph* g, int kind) {
+// Scratch a batched query needs: *own adds up over a batch (diamond per-arc counters), *shared
+// is charged once per batch at its largest (4-cycle counter and touched arrays of the owner
+// CTAs, within the slot's cap; edge-rooted lists of the heavy roots).  The DAG and the
+// 4-cycle apex classes count as graph bytes once built.
+void estimate_frontier(const jgpm_server* s, const jgpm_graph* g, int kind, uint64_t* own,
+                       uint64_t* shared) {
   const uint64_t sms = (uint64_t)device_sm_count(s->cfg.device);
+  const uint64_t grid = sms * 4;
+  *own = 0;
+  *shared = 0;
+  const uint64_t m_dag = g->m_dag > 0 ? (uint64_t)g->m_dag : (uint64_t)g->m / 2;
   if (kind == kJobC4) {
-    const uint64_t cap = std::max<uint64_t>((uint64_t)64 << 20,
-                                            s->cfg.memory_budget_bytes / 8 /
-                                                std::max(1, s->cfg.max_inflight));
-    return std::min<uint64_t>(cap, sms * 8 * (uint64_t)g->n * 4);
+    const uint64_t cap = s->slots.empty() ? ((uint64_t)4 << 30) : s->slots[0]->ctx.c4_cap_bytes;
+    *shared = 2 * std::min<uint64_t>(cap, grid * (uint64_t)g->n * 4);
+  } else {
+    if (kind == kJobDiamond) *own = m_dag * 4 + 256;
+    const int maxo = g->max_out_degree > 0 ? g->max_out_degree : g->max_degree;
+    if (maxo > kBatchCtaMaxDeg) {  // wide roots: bitmap rows per CTA
+      const uint64_t wd = (uint64_t)std::min(maxo, kBatchWideMaxDeg);
+      *shared += grid * wd * ((wd + 31) / 32) * 4;
+    }
+    if (maxo > kBatchWideMaxDeg) *shared += grid * 8 * 6 * ((uint64_t)maxo + 32) * 4;
   }
-  if (kind == kJobClique && g->tiers.large_end > 0)
-    return sms * 8 * 8 * 6 * ((uint64_t)g->max_out_degree + 32) * 4;
-  return 0;
 }
 
 bool pattern_known(const std::string& p, int induced) {
@@ -425,9 +460,14 @@ int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, ui
   }
   q->graph_id = graph_id;
   const jgpm_graph* g = s->graphs[graph_id].g;
-  q->frontier = q->plain ? (uint64_t)g->m_dag * 4 + (uint64_t)g->n * 8 + ((uint64_t)256 << 20)
-                         : estimate_frontier(s, g, q->kind);
-  if (q->frontier + s->graphs[graph_id].bytes > s->cfg.memory_budget_bytes) {
+  if (q->plain) {
+    const uint64_t m_dag = g->m_dag > 0 ? (uint64_t)g->m_dag : (uint64_t)g->m / 2;
+    q->frontier = m_dag * 4 + (uint64_t)g->n * 8 + ((uint64_t)256 << 20);
+  } else {
+    estimate_frontier(s, g, q->kind, &q->fr_own, &q->fr_shared);
+  }
+  const uint64_t need = q->plain ? q->frontier : q->fr_own + q->fr_shared;
+  if (need + s->graphs[graph_id].bytes > s->cfg.memory_budget_bytes) {
     s->st.rejected++;
     jgpm_set_error_("jgpm_server_submit: query frontier + graph exceed the memory budget");
     return JGPM_EADMISSION;

@@ -127,3 +127,29 @@ def test_batch_large_roots_complete_graph(gpu, mixed):
                 assert c == closed[p], p
             else:
                 assert c == want[(gs.index(g), p)], (gs.index(g), p)
+
+
+def test_batch_list_roots_crown(gpu, mixed):
+    """Roots of out-degree 5000 (above the batched bitmap limits) run on edge-rooted lists in
+    the batch: the crown graph of test_gpu_parity (closed forms), batched with small graphs."""
+    from math import comb
+    specs, gs, want = mixed
+    na, nb, g = 5000, 5001, 1250
+    a = np.arange(na, dtype=np.int64)
+    b = np.arange(na, na + nb, dtype=np.int64)
+    h = na + nb
+    grp = a.reshape(g, 4)
+    iu = np.triu_indices(4, 1)
+    s = np.concatenate([np.repeat(a, nb), np.full(na, h), grp[:, iu[0]].ravel()]).astype(np.int32)
+    d = np.concatenate([np.tile(b, na), a, grp[:, iu[1]].ravel()]).astype(np.int32)
+    with gpu.Graph.from_edges(s, d, h + 1) as crown:
+        closed = {"triangle": 4 * g + 6 * g + 6 * g * nb, "4-clique": g + 4 * g + 4 * g * nb,
+                  "5-clique": g * (1 + nb),
+                  "diamond": 3 * (na + na * nb) + 6 * g * comb(nb + 3, 2)}
+        jobs = [(crown, p) for p in closed] + [(gg, "4-clique") for gg in gs[:3]]
+        counts, _ = gpu.batch_count(jobs)
+        for (gg, p), c in zip(jobs, counts):
+            if gg is crown:
+                assert c == closed[p], p
+            else:
+                assert c == want[(gs.index(gg), p)]
