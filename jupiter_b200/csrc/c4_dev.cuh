@@ -235,7 +235,7 @@ __device__ __forceinline__ acc_t c4_large_apex(const eid_t* rp, const vid_t* col
                                                int32_t* dense, vid_t* touched,
                                                C4LargeSmem& sh) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nth = blockDim.x, nw = nth >> 5;
+  const int nth = blockDim.x;
   const eid_t b = rp[v];
   const int d = (int)(rp[v + 1] - b);
   if (tid == 0) {

@@ -41,6 +41,17 @@ __device__ __forceinline__ void count_below2(const int* a, int n, int top, int x
   }
 }
 
+// Position of the r-th set bit (r counted from 0) of the W-word row.
+__device__ __forceinline__ int select_bit(const uint32_t* row, int W, int r) {
+  for (int q = 0; q < W; ++q) {
+    const uint32_t w = row[q];
+    const int c = __popc(w);
+    if (r < c) return q * 32 + (int)__fns(w, 0, r + 1);
+    r -= c;
+  }
+  return 0;  // not reached: r < popc(row)
+}
+
 // ---------------------------------------------------------------- single-word rows
 template <int D, bool STATS>
 struct SmallCount {
@@ -362,7 +373,48 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
   }
   __syncwarp();
   acc_t cnt = 0;
-  for (int i = lane; i < d; i += 32) {
+  if (K >= 5 && !ETRI) {
+    // k >= 5: the first two levels flattened over the lanes as (row i, bit j of R_i) pairs,
+    // so one dense row does not hold up the warp.  off[i] = pairs before row i.
+    const int b0 = min(d, lane * kWarpW), b1 = min(d, b0 + kWarpW);
+    int local = 0;
+    for (int i = b0; i < b1; ++i) {
+      int c = 0;
+      for (int q = 0; q < w_d; ++q) c += __popc(ws.R[i * w_d + q]);
+      ws.off[i] = c;
+      local += c;
+    }
+    int incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    int run = incl - local;
+    for (int i = b0; i < b1; ++i) {
+      const int c = ws.off[i];
+      ws.off[i] = run;
+      run += c;
+    }
+    if (lane == 31) ws.off[d] = incl;
+    __syncwarp();
+    const int P = ws.off[d];
+    for (int p = lane; p < P; p += 32) {
+      int i, i2;
+      count_below2(ws.off + 1, d - 1, topO, p + 1, p + 1, i, i2);
+      const uint32_t* Ri = ws.R + i * w_d;
+      const int j = select_bit(Ri, w_d, p - ws.off[i]);
+      const uint32_t* Rj = ws.R + j * w_d;
+      uint32_t m2[kWarpW];
+#pragma unroll
+      for (int q = 0; q < kWarpW; ++q) m2[q] = q < w_d ? (Ri[q] & Rj[q]) : 0u;
+      if (STATS) elems += (acc_t)(ws.off[i + 1] - ws.off[i]) + (acc_t)ws.deg[j];
+      cnt += RowCount<(K >= 5 ? K - 4 : 1), kWarpW, STATS>::run(m2, ws.R, w_d, ws.deg, elems);
+    }
+    __syncwarp();
+    return cnt;
+  }
+  for (int i = lane; i < d && !(K >= 5 && !ETRI); i += 32) {
     uint32_t m[kWarpW];
 #pragma unroll
     for (int q = 0; q < kWarpW; ++q) m[q] = q < w_d ? ws.R[i * w_d + q] : 0u;
@@ -537,7 +589,54 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
   acc_t cnt = 0;
   static_assert(!GR || ROWW == 0, "rows in global memory are counted warp-cooperatively");
   constexpr int RW = ROWW > 0 ? ROWW : 1;
-  if (ROWW > 0 && w_d <= ROWW) {
+  if (ROWW > 0 && w_d <= ROWW && K >= 5 && !ETRI) {
+    // k >= 5: the first two levels flattened over the threads as (row i, bit j of R_i)
+    // pairs, so one dense row does not hold up the CTA.  off[i] = pairs before row i.
+    for (int i = tid; i < d; i += nthreads) {
+      int c = 0;
+      for (int q = 0; q < w_d; ++q) c += __popc(R[(size_t)i * w_d + q]);
+      off[i] = c;
+    }
+    __syncthreads();
+    {  // exclusive scan of off[0..d): blocked per thread, then across warps
+      const int per = (d + nthreads - 1) / nthreads;
+      const int b0 = min(d, tid * per), b1 = min(d, b0 + per);
+      int local = 0;
+      for (int i = b0; i < b1; ++i) local += off[i];
+      int incl = local;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane == 31) sm.wsum[warp] = incl;
+      __syncthreads();
+      int wbase = 0;
+      for (int w = 0; w < warp; ++w) wbase += sm.wsum[w];
+      int run = wbase + incl - local;
+      __syncthreads();
+      for (int i = b0; i < b1; ++i) {
+        const int l = off[i];
+        off[i] = run;
+        run += l;
+      }
+      if (tid == nthreads - 1) off[d] = run;
+      __syncthreads();
+    }
+    const int P = off[d];
+    for (int p = tid; p < P; p += nthreads) {
+      int i, i2;
+      count_below2(off + 1, d - 1, topO, p + 1, p + 1, i, i2);
+      const uint32_t* Ri = R + (size_t)i * w_d;
+      const int j = select_bit(Ri, w_d, p - off[i]);
+      const uint32_t* Rj = R + (size_t)j * w_d;
+      uint32_t m2[RW];
+#pragma unroll
+      for (int q = 0; q < RW; ++q) m2[q] = q < w_d ? (Ri[q] & Rj[q]) : 0u;
+      if (STATS) elems += (acc_t)(off[i + 1] - off[i]) + (acc_t)deg[j];
+      cnt += RowCount<(K >= 5 ? K - 4 : 1), RW, STATS>::run(m2, R, w_d, deg, elems);
+    }
+  } else if (ROWW > 0 && w_d <= ROWW) {
     // row-parallel: each thread owns rows, masks in registers
     for (int i = tid; i < d; i += nthreads) {
       uint32_t m[RW];
