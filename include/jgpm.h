@@ -65,7 +65,7 @@ typedef struct {
 #define JGPM_METHOD_BITMAP_CLIQUE 1  /* vertex-rooted local-bitmap k-clique kernels */
 #define JGPM_METHOD_PLAN 2           /* per-root nested-loop plan kernel */
 #define JGPM_METHOD_WEDGE 3          /* wedge aggregation (4-cycle) */
-#define JGPM_METHOD_EDGE_TRIANGLE 4  /* per-edge triangle counts (diamond, census) */
+#define JGPM_METHOD_EDGE_TRIANGLE 4  /* per-arc triangle counters (diamond, tailed triangle) */
 #define JGPM_METHOD_CENSUS 5         /* vertex-induced counts from the 4-vertex census */
 
 #define JGPM_COUNT_STATS 1u          /* also compute setop_elements (an extra untimed pass) */
@@ -189,13 +189,16 @@ typedef struct {
 
 typedef struct {
   double kernel_ms;       /* device time of the batch (task upload + kernel + count read-back) */
-  int32_t launches;       /* kernels launched (1: one persistent launch for the whole batch) */
+  int32_t launches;       /* kernels launched: the persistent task kernel, plus a second
+                             persistent kernel for large 4-cycle apexes when there are any */
   int32_t tasks;          /* tasks in the global queue */
   jgpm_tuning used;
 } jgpm_batch_stats;
 
-/* Counts every job exactly in ONE persistent work-stealing launch: all jobs' work is cut into
- * tasks of one global queue that persistent CTAs drain; counts[i] receives job i's count.
+/* Counts every job exactly in one persistent work-stealing launch: all jobs' work is cut into
+ * tasks of one global queue that persistent CTAs drain; counts[i] receives job i's count.  The
+ * large 4-cycle apexes of all jobs form a second queue, drained concurrently by a second
+ * persistent kernel with wider CTAs.
  * Replaces, for a whole batch, the reference's per-query round loop and static chunking
  * (src/jupiter_gpm.cu:356-375).  tuning = NULL uses the defaults.  All graphs must be on one
  * device. */

@@ -20,7 +20,9 @@
 //   C4_LARGE    one heavy 4-cycle apex on the whole CTA (dense counters in global memory).
 // Diamond jobs (reference P2, sum over edges of C(t_e, 2)) run the k = 3 root tasks in pair
 // mode: every triangle increments its three arcs' counters in the job's tri[] array and the
-// adds' old values give the pairs, so the count comes out of the same single pass.
+// adds' old values give the pairs, so the count comes out of the same single pass.  Jobs for
+// the vertex-induced tailed triangle ("induced:tailed-triangle") run the k = 4 tasks in TT
+// mode, 12 K4 - 4 N(diamond) + N(tailed triangle), in one pass as well.
 //
 // Resources: one kernel holds every task kind, so its registers and shared memory are the
 // largest any kind needs.  The CTA roots count warp-cooperatively (masks one word per lane)
@@ -50,15 +52,10 @@ namespace jgpm {
 
 struct BatchArgs {
   const JobDesc* jobs;
-  const Task* tasks;     // [0, n_c4): large 4-cycle apexes; [n_c4, ntasks): all others
+  const Task* tasks;
   int64_t ntasks;
-  int64_t n_c4;
-  int c4_ctas;           // CTAs [0, c4_ctas) own a dense counter array and drain the apex queue
   unsigned long long* counts;
-  unsigned long long* cursor;  // [0] main queue, [1] large-apex queue
-  int32_t* c4_counters;  // per owner CTA: c4_stride counters, zero between apexes
-  vid_t* c4_touched;      // per owner CTA: c4_stride touched ids
-  int64_t c4_stride;
+  unsigned long long* cursor;  // [0] task queue
   int32_t* list_scratch;  // per warp: kLevels lists of list_cap ints
   int64_t list_cap;
   int dmax, W;            // CTA-root bitmap layout
@@ -114,7 +111,7 @@ struct BatchListClique {
   }
 };
 
-template <int G, int K, bool PAIRS>
+template <int G, int K, bool PAIRS, bool TT = false>
 __device__ __forceinline__ acc_t task_groups(const JobDesc& j, int64_t b, int64_t e,
                                              uint32_t* rows, int* degs) {
   constexpr int kGroups = 32 / G;
@@ -127,7 +124,8 @@ __device__ __forceinline__ acc_t task_groups(const JobDesc& j, int64_t b, int64_
   for (int64_t first = b + (int64_t)warp * kGroups; first < e; first += 8 * kGroups) {
     const int64_t idx = first + gi;
     const vid_t u = idx < e ? j.roots[idx] : -1;
-    cnt += group_root<G, K, false, PAIRS, PAIRS>(j.drow, j.dcol, u, R, DG, j.tri, el);
+    cnt += group_root<G, K, false, PAIRS, PAIRS, TT>(j.drow, j.dcol, u, R, DG, j.tri, el,
+                                                     j.srow);
   }
   return cnt;
 }
@@ -136,6 +134,7 @@ template <int G>
 __device__ __forceinline__ acc_t task_groups_k(const JobDesc& j, int64_t b, int64_t e,
                                                uint32_t* rows, int* degs) {
   if (j.kind == kJobDiamond) return task_groups<G, 3, true>(j, b, e, rows, degs);
+  if (j.kind == kJobIndTT) return task_groups<G, 4, true, true>(j, b, e, rows, degs);
   switch (j.k) {
     case 3: return task_groups<G, 3, false>(j, b, e, rows, degs);
     case 4: return task_groups<G, 4, false>(j, b, e, rows, degs);
@@ -146,18 +145,20 @@ __device__ __forceinline__ acc_t task_groups_k(const JobDesc& j, int64_t b, int6
   }
 }
 
-template <int K, bool PAIRS>
+template <int K, bool PAIRS, bool TT = false>
 __device__ __forceinline__ acc_t warp_roots_k(const JobDesc& j, int64_t b, int64_t e,
                                               WarpSmem& ws) {
   acc_t cnt = 0, el = 0;
   for (int64_t r = b + (threadIdx.x >> 5); r < e; r += 8)
-    cnt += warp_root<K, false, PAIRS, PAIRS>(j.drow, j.dcol, j.roots[r], ws, j.tri, el);
+    cnt += warp_root<K, false, PAIRS, PAIRS, TT>(j.drow, j.dcol, j.roots[r], ws, j.tri, el,
+                                                 j.srow);
   return cnt;
 }
 
 __device__ __forceinline__ acc_t task_warp_roots(const JobDesc& j, int64_t b, int64_t e,
                                                  WarpSmem& ws) {
   if (j.kind == kJobDiamond) return warp_roots_k<3, true>(j, b, e, ws);
+  if (j.kind == kJobIndTT) return warp_roots_k<4, true, true>(j, b, e, ws);
   switch (j.k) {
     case 3: return warp_roots_k<3, false>(j, b, e, ws);
     case 4: return warp_roots_k<4, false>(j, b, e, ws);
@@ -172,6 +173,9 @@ __device__ __forceinline__ acc_t task_cta_root(const JobDesc& j, vid_t u, const 
   acc_t el = 0;
   if (j.kind == kJobDiamond)
     return cta_root<3, false, true, true, 0>(j.drow, j.dcol, u, sm, j.tri, el);
+  if (j.kind == kJobIndTT)
+    return cta_root<4, false, true, true, 0, 1, false, true>(j.drow, j.dcol, u, sm, j.tri, el,
+                                                             j.srow);
   switch (j.k) {
     case 3: return cta_root<3, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
     case 4: return cta_root<4, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
@@ -187,6 +191,9 @@ __device__ __forceinline__ acc_t task_wide_root(const JobDesc& j, vid_t u, const
   acc_t el = 0;
   if (j.kind == kJobDiamond)
     return cta_root<3, false, true, true, 0, 2, true>(j.drow, j.dcol, u, sm, j.tri, el);
+  if (j.kind == kJobIndTT)
+    return cta_root<4, false, true, true, 0, 2, true, true>(j.drow, j.dcol, u, sm, j.tri, el,
+                                                            j.srow);
   switch (j.k) {
     case 3: return cta_root<3, false, false, false, 0, 2, true>(j.drow, j.dcol, u, sm, nullptr, el);
     case 4: return cta_root<4, false, false, false, 0, 2, true>(j.drow, j.dcol, u, sm, nullptr, el);
@@ -216,14 +223,27 @@ __device__ acc_t task_large_root(const JobDesc& j, vid_t u, const BatchArgs& a) 
     const int dv = (int)(j.drow[v + 1] - bv);
     const int tw = warp_intersect(j.dcol + bu, du, j.dcol + bv, dv, INT32_MAX, buf);
     if (tw == 0) continue;
-    if (j.kind == kJobDiamond) {
-      if (lane == 0) cnt += pair_gain(atomicAdd(j.tri + bu + i, (unsigned)tw), (unsigned)tw);
+    if (j.kind == kJobDiamond || j.kind == kJobIndTT) {
+      // pair gains (weight 1 for diamond, -4 in the tailed-triangle value) and, for the
+      // tailed triangle, the degree terms of the triangles (u, v, w) and 12 x the 4-cliques
+      const bool tt = j.kind == kJobIndTT;
+      const acc_t pw = tt ? (acc_t)0 - 4ull : 1ull;
+      if (lane == 0)
+        cnt += pw * pair_gain(atomicAdd(j.tri + bu + i, (unsigned)tw), (unsigned)tw);
+      const acc_t tuv = tt ? tt_deg(j.srow, u) + tt_deg(j.srow, v) : 0ull;
       for (int q = lane; q < tw; q += 32) {
         const vid_t w = buf[q];
-        cnt += (acc_t)atomicAdd(j.tri + bu + lower_bound_g(j.dcol + bu, du, w), 1u);
-        cnt += (acc_t)atomicAdd(j.tri + bv + lower_bound_g(j.dcol + bv, dv, w), 1u);
+        acc_t o = (acc_t)atomicAdd(j.tri + bu + lower_bound_g(j.dcol + bu, du, w), 1u);
+        o += (acc_t)atomicAdd(j.tri + bv + lower_bound_g(j.dcol + bv, dv, w), 1u);
+        cnt += pw * o;
+        if (tt) cnt += tuv + tt_deg(j.srow, w);
       }
       __syncwarp();
+      if (tt) {
+        const acc_t k4 = BatchListClique<1>::run(j.drow, j.dcol, buf, tw, buf + cap, cap,
+                                                 a.intersect);
+        if (lane == 0) cnt += 12ull * k4;
+      }
       continue;
     }
     acc_t c = (acc_t)tw;
@@ -259,28 +279,14 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
   __shared__ uint32_t rows[256];
   __shared__ int degs[256];
   __shared__ unsigned long long s_task;
-  __shared__ C4LargeSmem s_c4l;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  const bool c4_owner = a.c4_counters && (int)blockIdx.x < a.c4_ctas;
-  int32_t* c4 = c4_owner ? a.c4_counters + (int64_t)blockIdx.x * a.c4_stride : nullptr;
-  vid_t* c4t = c4_owner ? a.c4_touched + (int64_t)blockIdx.x * a.c4_stride : nullptr;
-  bool c4_done = !c4_owner;
   int smem_kind = -1;  // which layout the dynamic shared memory holds (hash tables persist)
   for (;;) {
-    if (tid == 0) {
-      unsigned long long t = ~0ull;
-      if (!c4_done) {
-        t = atomicAdd(&a.cursor[1], 1ull);
-        if ((int64_t)t >= a.n_c4) t = ~0ull;
-      }
-      if (t == ~0ull) t = (unsigned long long)a.n_c4 + atomicAdd(&a.cursor[0], 1ull);
-      s_task = t;
-    }
+    if (tid == 0) s_task = atomicAdd(&a.cursor[0], 1ull);
     __syncthreads();
     const int64_t ti = (int64_t)s_task;
     __syncthreads();
-    if (ti >= a.n_c4) c4_done = true;
     if (ti >= a.ntasks) break;
     const Task t = a.tasks[ti];
     const JobDesc j = a.jobs[t.job];
@@ -320,12 +326,44 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
         }
         for (int64_t q = t.b; q < t.e; ++q) c += c4_mid_apex(j.rrow, j.rcol, j.mid[q], cta_hash);
         break;
-      case kTaskC4Large:
-        c = c4_large_apex(j.rrow, j.rcol, j.apexes[t.b], c4, c4t, s_c4l);
-        break;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
     if (lane == 0 && c) atomicAdd(&a.counts[t.job], c);
+  }
+}
+
+// Large 4-cycle apexes of every 4-cycle job of the batch, heaviest first, on CTAs of 1024
+// threads with one dense counter array (and touched list) of stride ints each; launched next
+// to k_batch on a second stream.
+struct C4BatchArgs {
+  const JobDesc* jobs;
+  const Task* tasks;  // (job, apex index b)
+  int64_t ntasks;
+  unsigned long long* counts;
+  unsigned long long* cursor;
+  int32_t* dense;
+  vid_t* touched;
+  int64_t stride;
+};
+
+constexpr int kBatchC4Threads = 1024;
+
+__global__ void __launch_bounds__(kBatchC4Threads) k_batch_c4_large(C4BatchArgs a) {
+  __shared__ C4LargeSmem<kBatchC4Threads> sh;
+  __shared__ unsigned long long s_q;
+  int32_t* dense = a.dense + (int64_t)blockIdx.x * a.stride;
+  vid_t* touched = a.touched + (int64_t)blockIdx.x * a.stride;
+  for (;;) {
+    if (threadIdx.x == 0) s_q = atomicAdd(a.cursor, 1ull);
+    __syncthreads();
+    const int64_t q = (int64_t)s_q;
+    __syncthreads();
+    if (q >= a.ntasks) break;
+    const Task t = a.tasks[q];
+    const JobDesc j = a.jobs[t.job];
+    acc_t c = c4_large_apex(j.rrow, j.rcol, j.apexes[t.b], dense, touched, sh);
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(&a.counts[t.job], c);
   }
 }
 
@@ -365,6 +403,7 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
   c.h_jobs.clear();
   c.h_tasks.clear();
   std::vector<Task> heavy, cta, warp, c4m, c4s, light, c4l;
+  std::vector<uint64_t> c4w;  // wedge bound of each large-apex task
   std::vector<size_t> tri_off(in.size(), 0);
   const int split = tu.split_degree >= 128 ? 128 : tu.split_degree >= 64 ? 64 : 32;
   const int64_t rpt = std::max(8, tu.roots_per_task);
@@ -374,7 +413,7 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
     JobDesc jd{};
     jd.n = g->n;
     jd.kind = in[ji].kind;
-    jd.k = in[ji].kind == kJobDiamond ? 3 : in[ji].k;
+    jd.k = in[ji].kind == kJobDiamond ? 3 : in[ji].kind == kJobIndTT ? 4 : in[ji].k;
     const int job = (int)ji;
     if (in[ji].kind == kJobC4) {
       if ((rc = ensure_c4_apexes(g))) return rc;
@@ -383,7 +422,10 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
       jd.roots = g->d_c4_small;
       jd.apexes = g->d_c4_large;
       jd.mid = g->d_c4_mid;
-      for (int64_t q = 0; q < g->c4_nlarge; ++q) c4l.push_back(Task{job, kTaskC4Large, q, q + 1});
+      for (int64_t q = 0; q < g->c4_nlarge; ++q) {
+        c4l.push_back(Task{job, kTaskC4Large, q, q + 1});
+        c4w.push_back(g->c4_large_keys[(size_t)q]);
+      }
       if (g->c4_nlarge > 0) o->c4max = std::max<int64_t>(o->c4max, g->n);
       add_range_tasks(c4m, job, kTaskC4Mid, 0, g->c4_nmid, 2);
       add_range_tasks(c4s, job, kTaskC4Small, 0, g->c4_nsmall, std::max<int64_t>(8, rpt / 8));
@@ -396,11 +438,14 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
     jd.dcol = g->d_dag_col;
     const RootTiers& t = g->tiers;
     jd.roots = t.d_roots;
-    if (in[ji].kind == kJobDiamond) {
+    jd.srow = g->d_rowptr;
+    const bool per_arc = in[ji].kind == kJobDiamond || in[ji].kind == kJobIndTT;
+    if (per_arc) {
       tri_off[ji] = o->tri_bytes;
       o->tri_bytes += ((size_t)std::max<int64_t>(1, g->m_dag) * 4 + 255) & ~(size_t)255;
     }
-    const int64_t stop = t.deg_begin[jd.k - 2];  // roots with d >= k-1
+    // roots with d >= k-1; every triangle's root (d >= 2) for the per-arc counter jobs
+    const int64_t stop = t.deg_begin[per_arc ? 1 : jd.k - 2];
     // roots by out-degree: > 2048 large | (512, 2048] wide | (split, 512] CTA |
     // (32, split] warp | <= 32 groups
     const int64_t wide_begin = std::min(stop, t.le_begin[5]);
@@ -436,12 +481,21 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
     }
     c.h_jobs.push_back(jd);
   }
-  // heaviest first: large apexes (own queue), large roots, CTA roots, mid apexes, warp
-  // roots, small apexes, lane groups
-  c.n_c4 = (int64_t)c4l.size();
-  c.h_tasks.reserve(c4l.size() + heavy.size() + cta.size() + c4m.size() + warp.size() +
-                    c4s.size() + light.size());
-  for (auto* v : {&c4l, &heavy, &cta, &c4m, &warp, &c4s, &light})
+  // large 4-cycle apexes (all jobs', by descending wedge bound) go to k_batch_c4_large; the
+  // main queue: large roots, CTA roots, mid apexes, warp roots, small apexes, lane groups
+  if (c4l.size() > 1) {
+    std::vector<uint32_t> ord(c4l.size());
+    for (size_t q = 0; q < ord.size(); ++q) ord[q] = (uint32_t)q;
+    std::stable_sort(ord.begin(), ord.end(),
+                     [&](uint32_t x, uint32_t y) { return c4w[x] > c4w[y]; });
+    std::vector<Task> sorted(c4l.size());
+    for (size_t q = 0; q < ord.size(); ++q) sorted[q] = c4l[ord[q]];
+    c4l.swap(sorted);
+  }
+  c.h_c4_tasks.swap(c4l);
+  c.h_tasks.reserve(heavy.size() + cta.size() + c4m.size() + warp.size() + c4s.size() +
+                    light.size());
+  for (auto* v : {&heavy, &cta, &c4m, &warp, &c4s, &light})
     c.h_tasks.insert(c.h_tasks.end(), v->begin(), v->end());
   c.tri_off.swap(tri_off);
   return JGPM_OK;
@@ -452,7 +506,7 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
 // Enqueues one batched launch on `s`; per-job counts land in c.counts (device) and are
 // copied to `h_counts` (pinned or pageable host memory) on the same stream.
 int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tuning& tu,
-                  cudaStream_t s, uint64_t* h_counts, int* ntasks_out) {
+                  cudaStream_t s, uint64_t* h_counts, int* ntasks_out, int* launches_out) {
   BuildOut o;
   int rc;
   if ((rc = build_tasks(in, tu, c, &o))) return rc;
@@ -473,25 +527,11 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   if (o.tri_bytes) {
     if ((rc = c.tri.reserve(o.tri_bytes))) return rc;
     for (size_t ji = 0; ji < nj; ++ji)
-      if (c.h_jobs[ji].kind == kJobDiamond)
+      if (c.h_jobs[ji].kind == kJobDiamond || c.h_jobs[ji].kind == kJobIndTT)
         c.h_jobs[ji].tri = (uint32_t*)((char*)c.tri.p + c.tri_off[ji]);
     JGPM_CUDA_TRY(cudaMemsetAsync(c.tri.p, 0, o.tri_bytes, s));
   }
   BatchArgs a{};
-  if (o.c4max > 0) {
-    const size_t per_cta = (size_t)o.c4max * sizeof(int32_t);
-    a.c4_ctas = (int)std::max<size_t>(1, std::min<size_t>((size_t)grid, c.c4_cap_bytes / per_cta));
-    const size_t need = (size_t)a.c4_ctas * per_cta;
-    if ((rc = c.c4.reserve(need))) return rc;
-    if (c.c4_zeroed < need) {  // counters are zero between apexes; zero fresh memory once
-      JGPM_CUDA_TRY(cudaMemsetAsync(c.c4.p, 0, c.c4.bytes, s));
-      c.c4_zeroed = c.c4.bytes;
-    }
-    if ((rc = c.c4t.reserve(need))) return rc;
-    a.c4_counters = (int32_t*)c.c4.p;
-    a.c4_touched = (vid_t*)c.c4t.p;
-    a.c4_stride = o.c4max;
-  }
   if (o.wdmax > 0) {
     if ((rc = c.rows.reserve((size_t)grid * o.wdmax * wW * sizeof(uint32_t)))) return rc;
     a.rows = (uint32_t*)c.rows.p;
@@ -511,10 +551,44 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
                                   cudaMemcpyHostToDevice, s));
   JGPM_CUDA_TRY(cudaMemsetAsync(c.counts.p, 0, nj * sizeof(unsigned long long), s));
   JGPM_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, 2 * sizeof(unsigned long long), s));
+  // large 4-cycle apexes: k_batch_c4_large on the side stream, concurrently with k_batch
+  const size_t n4 = c.h_c4_tasks.size();
+  bool forked = false;
+  if (n4 > 0) {
+    const size_t per_cta = (size_t)o.c4max * sizeof(int32_t);
+    const int64_t ctas = std::max<int64_t>(
+        1, std::min<int64_t>(std::min<int64_t>((int64_t)sms * 2, (int64_t)n4),
+                             (int64_t)(c.c4_cap_bytes / std::max<size_t>(1, per_cta))));
+    const size_t need = (size_t)ctas * per_cta;
+    if ((rc = c.c4.reserve(need))) return rc;
+    if (c.c4_zeroed < need) {  // counters are zero between apexes; zero fresh memory once
+      JGPM_CUDA_TRY(cudaMemsetAsync(c.c4.p, 0, c.c4.bytes, s));
+      c.c4_zeroed = c.c4.bytes;
+    }
+    if ((rc = c.c4t.reserve(need))) return rc;
+    if ((rc = c.c4_tasks.reserve(n4 * sizeof(Task)))) return rc;
+    JGPM_CUDA_TRY(cudaMemcpyAsync(c.c4_tasks.p, c.h_c4_tasks.data(), n4 * sizeof(Task),
+                                  cudaMemcpyHostToDevice, s));
+    if ((rc = c.ensure_side_stream())) return rc;
+    JGPM_CUDA_TRY(cudaEventRecord(c.fork_ev, s));
+    JGPM_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork_ev, 0));
+    C4BatchArgs b{};
+    b.jobs = (const JobDesc*)c.jobs.p;
+    b.tasks = (const Task*)c.c4_tasks.p;
+    b.ntasks = (int64_t)n4;
+    b.counts = (unsigned long long*)c.counts.p;
+    b.cursor = (unsigned long long*)c.cursor.p + 1;
+    b.dense = (int32_t*)c.c4.p;
+    b.touched = (vid_t*)c.c4t.p;
+    b.stride = o.c4max;
+    k_batch_c4_large<<<(int)ctas, kBatchC4Threads, 0, c.side>>>(b);
+    JGPM_CUDA_TRY(cudaGetLastError());
+    JGPM_CUDA_TRY(cudaEventRecord(c.join_ev, c.side));
+    forked = true;
+  }
   a.jobs = (const JobDesc*)c.jobs.p;
   a.tasks = (const Task*)c.tasks.p;
   a.ntasks = (int64_t)nt;
-  a.n_c4 = c.n_c4;
   a.counts = (unsigned long long*)c.counts.p;
   a.cursor = (unsigned long long*)c.cursor.p;
   a.dmax = o.dmax;
@@ -522,10 +596,12 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   a.intersect = tu.intersect;
   if (nt) k_batch<<<grid, 256, smem, s>>>(a);
   JGPM_CUDA_TRY(cudaGetLastError());
+  if (forked) JGPM_CUDA_TRY(cudaStreamWaitEvent(s, c.join_ev, 0));
   if (h_counts)
     JGPM_CUDA_TRY(cudaMemcpyAsync(h_counts, c.counts.p, nj * sizeof(uint64_t),
                                   cudaMemcpyDeviceToHost, s));
-  if (ntasks_out) *ntasks_out = (int)nt;
+  if (ntasks_out) *ntasks_out = (int)(nt + n4);
+  if (launches_out) *launches_out = (nt ? 1 : 0) + (n4 ? 1 : 0);
   return JGPM_OK;
 }
 
@@ -542,6 +618,7 @@ int parse_batch_pattern(const char* pattern, int* kind, int* k) {
     *k = atoi(p.c_str() + 9);
     if (*k < 3 || *k > 8) return JGPM_EPATTERN;
   } else if (p == "diamond" || p == "P2") { *kind = kJobDiamond; }
+  else if (p == "induced:tailed-triangle") { *kind = kJobIndTT; *k = 4; }
   else if (p == "4-cycle" || p == "P1") { *kind = kJobC4; }
   else return JGPM_EPATTERN;
   return JGPM_OK;
@@ -568,7 +645,8 @@ int collect_jobs(const jgpm_job* jobs, int32_t njobs, std::vector<BatchJobIn>& i
     if (parse_batch_pattern(jobs[i].pattern, &b.kind, &b.k)) {
       jgpm_set_error_("batch: job " + std::to_string(i) + ": pattern '" +
                       std::string(jobs[i].pattern ? jobs[i].pattern : "") +
-                      "' is not batchable (triangle, k-clique, diamond, 4-cycle)");
+                      "' is not batchable (triangle, k-clique, diamond, 4-cycle, "
+                      "induced:tailed-triangle)");
       return JGPM_EPATTERN;
     }
     if (i == 0) *device = jobs[i].graph->device;
@@ -635,12 +713,12 @@ int jgpm_batch_count(const jgpm_job* jobs, int32_t njobs, const jgpm_tuning* tun
   // every graph's own stream must be idle before the batch reads it
   for (int32_t i = 0; i < njobs; ++i) cudaStreamSynchronize(jobs[i].graph->stream);
   std::vector<uint64_t> h((size_t)njobs);
-  int ntasks = 0;
+  int ntasks = 0, launches = 0;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, s);
-  rc = batch_enqueue(c, in, tu, s, h.data(), &ntasks);
+  rc = batch_enqueue(c, in, tu, s, h.data(), &ntasks, &launches);
   cudaEventRecord(e1, s);
   cudaError_t ce = cudaStreamSynchronize(s);
   float ms = 0.f;
@@ -656,7 +734,7 @@ int jgpm_batch_count(const jgpm_job* jobs, int32_t njobs, const jgpm_tuning* tun
   memcpy(counts, h.data(), h.size() * sizeof(uint64_t));
   if (st) {
     st->kernel_ms = ms;
-    st->launches = ntasks > 0 ? 1 : 0;
+    st->launches = launches;
     st->tasks = ntasks;
     st->used = tu;
   }

@@ -13,6 +13,7 @@ enum BatchKind : int32_t {
   kJobClique = 0,
   kJobDiamond = 1,
   kJobC4 = 2,
+  kJobIndTT = 3,  // vertex-induced tailed triangle (k = 4 tasks in TT mode)
 };
 
 enum TaskKind : int32_t {
@@ -24,7 +25,7 @@ enum TaskKind : int32_t {
   kTaskCtaRoot = 5,    // root b, split < d <= kBatchCtaMaxDeg, the whole CTA
   kTaskLargeRoot = 6,  // root b, d > kBatchWideMaxDeg, warps take its arcs (edge-rooted lists)
   kTaskC4Small = 7,    // small 4-cycle apexes [b, e) of the job's list, one per warp
-  kTaskC4Large = 8,    // large 4-cycle apex b of the job's list, the whole CTA
+  kTaskC4Large = 8,    // large 4-cycle apex b of the job's list (k_batch_c4_large)
   kTaskC4Mid = 9,      // mid 4-cycle apexes [b, e) of the job's list, one after another per CTA
   kTaskWideRoot = 10,  // root b, kBatchCtaMaxDeg < d <= kBatchWideMaxDeg, the whole CTA with
                        // its bitmap rows in global scratch
@@ -45,7 +46,8 @@ struct JobDesc {
   const vid_t* roots;   // root tiers (descending out-degree), or the small 4-cycle apexes
   const vid_t* apexes;  // large 4-cycle apexes (descending wedge bound)
   const vid_t* mid;     // mid 4-cycle apexes
-  uint32_t* tri;        // diamond: per-arc triangle counters (zero at launch)
+  uint32_t* tri;        // diamond, tailed triangle: per-arc triangle counters (zero at launch)
+  const eid_t* srow;    // tailed triangle: symmetric row pointers (degrees)
   int32_t n;
   int32_t kind;
   int32_t k;
@@ -82,16 +84,33 @@ struct DevArena {
 // scratch).  One per server slot or per synchronous caller.
 struct BatchCtx {
   int device = 0;
-  DevArena jobs, tasks, counts, cursor, c4, c4t, lists, tri, rows;
+  DevArena jobs, tasks, counts, cursor, c4, c4t, lists, tri, rows, c4_tasks;
   std::vector<JobDesc> h_jobs;
   std::vector<Task> h_tasks;
-  int64_t n_c4 = 0;
+  std::vector<Task> h_c4_tasks;  // large 4-cycle apexes, heaviest first
+  cudaStream_t side = nullptr;   // second stream of the large-apex kernel
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   std::vector<size_t> tri_off;  // diamond jobs: offset of the job's counters in `tri`
   size_t c4_zeroed = 0;
   size_t c4_cap_bytes = (size_t)4 << 30;  // memory cap of the 4-cycle counter arrays
+  int ensure_side_stream() {
+    if (side) return JGPM_OK;
+    if (cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      jgpm_set_error_("batch: stream/event creation failed");
+      return JGPM_ECUDA;
+    }
+    return JGPM_OK;
+  }
   ~BatchCtx() {
-    for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &c4t, &lists, &tri, &rows})
+    for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &c4t, &lists, &tri, &rows,
+                        &c4_tasks})
       if (d->p) cudaFree(d->p);
+    if (side) cudaStreamDestroy(side);
+    if (fork_ev) cudaEventDestroy(fork_ev);
+    if (join_ev) cudaEventDestroy(join_ev);
   }
 };
 
@@ -104,6 +123,7 @@ struct BatchJobIn {
 int parse_batch_pattern(const char* pattern, int* kind, int* k);
 jgpm_tuning default_tuning();
 int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tuning& tu,
-                  cudaStream_t s, uint64_t* h_counts, int* ntasks_out);
+                  cudaStream_t s, uint64_t* h_counts, int* ntasks_out,
+                  int* launches_out = nullptr);
 
 }  // namespace jgpm

@@ -93,14 +93,17 @@ __global__ void __launch_bounds__(256) k_c4_mid(const eid_t* rp, const vid_t* co
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
 }
 
-__global__ void __launch_bounds__(256) k_c4_large(const eid_t* rp, const vid_t* col, vid_t n,
-                                                  const vid_t* list, int64_t nlist,
-                                                  unsigned long long* cursor, int32_t* counters,
-                                                  DevControl* ctl) {
+// 1024 threads per CTA: the dense arrays are large (n ints each), so each one is shared by as
+// many warps as a CTA holds, to keep enough atomics in flight.
+constexpr int kC4LargeThreads = 1024;
+
+__global__ void __launch_bounds__(kC4LargeThreads)
+    k_c4_large(const eid_t* rp, const vid_t* col, vid_t n, const vid_t* list, int64_t nlist,
+               unsigned long long* cursor, int32_t* counters, DevControl* ctl) {
   int32_t* dense = counters + (int64_t)blockIdx.x * 2 * n;  // n counters, then n touched ids
   vid_t* touched = dense + n;
   __shared__ unsigned long long s_q;
-  __shared__ C4LargeSmem sh;
+  __shared__ C4LargeSmem<kC4LargeThreads> sh;
   const int tid = threadIdx.x, lane = tid & 31;
   acc_t sum = 0;
   for (;;) {
@@ -189,6 +192,10 @@ int ensure_c4_apexes(jgpm_graph* g) {
         tmp.p, tb, (const uint64_t*)lkey.p, (uint64_t*)lkey2.p, (const vid_t*)large.p, dl,
         (int)nlarge, 0, 64, s));
   }
+  g->c4_large_keys.resize((size_t)nlarge);
+  if (nlarge)
+    JGPM_CUDA_TRY(cudaMemcpyAsync(g->c4_large_keys.data(), lkey2.p, (size_t)nlarge * 8,
+                                  cudaMemcpyDeviceToHost, s));
   JGPM_CUDA_TRY(cudaStreamSynchronize(s));
   g->c4_nsmall = nsmall;
   g->c4_nmid = nmid;
@@ -207,12 +214,14 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
   const int sms = device_sm_count(g->device);
   const int64_t nsmall = g->c4_nsmall, nmid = g->c4_nmid, nlarge = g->c4_nlarge;
   // dense counters and touched lists for the large apexes: 2n ints per CTA, within a 12 GiB
-  // cap
+  // cap.  They are allocated for this count only (a graph pool would otherwise keep one such
+  // array set per graph).
   const int64_t per_cta = (int64_t)n * 8;
   int64_t ctas = std::min<int64_t>((int64_t)sms * 2,
                                    ((int64_t)12 << 30) / std::max<int64_t>(1, per_cta));
   ctas = std::max<int64_t>(1, std::min<int64_t>(ctas, nlarge));
-  if (nlarge > 0 && (rc = ensure_scratch(g, (size_t)(ctas * per_cta)))) return rc;
+  TmpBuf dense;
+  if (nlarge > 0 && (rc = dense.alloc((size_t)(ctas * per_cta)))) return rc;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -241,10 +250,10 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
     g->launches += 1;
   }
   if (nlarge > 0) {
-    JGPM_CUDA_TRY(cudaMemsetAsync(g->d_scratch, 0, (size_t)(ctas * per_cta), s));
-    k_c4_large<<<(int)ctas, 256, 0, s>>>(g->d_rank_rowptr, g->d_rank_col, n,
+    JGPM_CUDA_TRY(cudaMemsetAsync(dense.p, 0, (size_t)(ctas * per_cta), s));
+    k_c4_large<<<(int)ctas, kC4LargeThreads, 0, s>>>(g->d_rank_rowptr, g->d_rank_col, n,
                                          g->d_c4_large, nlarge, &g->d_ctl->counter[1],
-                                         (int32_t*)g->d_scratch, g->d_ctl);
+                                         (int32_t*)dense.p, g->d_ctl);
     g->launches += 1;
   }
   cudaEventRecord(e1, s);

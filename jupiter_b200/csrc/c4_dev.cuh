@@ -204,12 +204,13 @@ __device__ __forceinline__ acc_t c4_mid_apex(const eid_t* rp, const vid_t* col, 
   return sum;
 }
 
-// Shared memory of the large-apex path (blockDim <= 256).
+// Shared memory of the large-apex path for CTAs of up to NT threads.
+template <int NT>
 struct C4LargeSmem {
   int cut, nt;
-  int off[257];   // exclusive offsets of the block's x wedge counts, off[256] = total
-  int wsum[8];
-  eid_t bx[256];  // start of prefix(N(x), v) for the block's x
+  int off[NT + 1];  // exclusive offsets of the block's x wedge counts, off[NT] = total
+  int wsum[NT / 32];
+  eid_t bx[NT];     // start of prefix(N(x), v) for the block's x
 };
 
 // Binary lifting over a sorted shared-memory array (fixed trip count, top = largest power of
@@ -231,9 +232,10 @@ __device__ __forceinline__ void c4_count_below2(const int* a, int n, int top, in
 // and appends each vertex counted for the first time to the touched list; pass 1 reads and
 // clears only the touched counters.  Every thread calls it.  Returns this thread's share of
 // sum C(c, 2).
+template <int NT>
 __device__ __forceinline__ acc_t c4_large_apex(const eid_t* rp, const vid_t* col, vid_t v,
                                                int32_t* dense, vid_t* touched,
-                                               C4LargeSmem& sh) {
+                                               C4LargeSmem<NT>& sh) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nth = blockDim.x;
   const eid_t b = rp[v];

@@ -11,7 +11,14 @@
 //   PAIRS  ETRI whose adds return the old value; an add of k to a counter holding o creates
 //          k*o + C(k, 2) new pairs of triangles on that edge, so the sum over all adds is
 //          sum_e C(t_e, 2) -- the diamond count -- in one pass (tri[] starts at zero).
-//   The root kernels return the pair count in PAIRS mode and the clique count otherwise.
+//   TT     (k = 4, with ETRI and PAIRS) the vertex-induced tailed-triangle count in the same
+//          pass: I(TT) = N(TT) - 4 N(diamond) + 12 K4, where N(TT) = sum over triangles of
+//          (d_a - 2) + (d_b - 2) + (d_c - 2) with d the symmetric degree (srow).  Each root
+//          returns 12 K4 - 4 pairs + its triangles' degree terms in wrapping 64-bit
+//          arithmetic; the sum over all roots is the exact (non-negative) count.
+//   The root kernels return the pair count in PAIRS mode, the TT value in TT mode and the
+//   clique count otherwise.
+
 #pragma once
 #include "jgpm_internal.h"
 #include "setops.cuh"
@@ -21,6 +28,11 @@ namespace jgpm {
 // Pairs of triangles created on one edge by adding k to a counter that held o.
 __device__ __forceinline__ acc_t pair_gain(unsigned o, unsigned k) {
   return (acc_t)k * (acc_t)o + (acc_t)k * (acc_t)(k - 1) / 2;
+}
+
+// Symmetric degree minus two (the tailed-triangle degree term of a triangle vertex).
+__device__ __forceinline__ acc_t tt_deg(const eid_t* srow, vid_t v) {
+  return (acc_t)(srow[v + 1] - srow[v]) - 2ull;
 }
 
 constexpr int kRangeCut = 32;  // restrict a row to [L0, Ld-1] when longer than this
@@ -50,6 +62,15 @@ __device__ __forceinline__ int select_bit(const uint32_t* row, int W, int r) {
     r -= c;
   }
   return 0;  // not reached: r < popc(row)
+}
+
+// Word w of a register array, by an unrolled select (the array stays in registers).
+template <int WMAX>
+__device__ __forceinline__ uint32_t pick_word(const uint32_t (&m)[WMAX], int w) {
+  uint32_t r = 0u;
+#pragma unroll
+  for (int q = 0; q < WMAX; ++q) r = (q == w) ? m[q] : r;
+  return r;
 }
 
 // ---------------------------------------------------------------- single-word rows
@@ -82,11 +103,11 @@ struct SmallCount<0, STATS> {
 // with its group's root u (or u < 0 for an idle group).  R and DG point at the group's G
 // shared words.  Returns this lane's partial count.  tri (edge-triangle mode) receives one
 // count per triangle arc.
-template <int G, int K, bool STATS, bool ETRI, bool PAIRS = false>
+template <int G, int K, bool STATS, bool ETRI, bool PAIRS = false, bool TT = false>
 __device__ __forceinline__ acc_t group_root(const eid_t* __restrict__ rowptr,
                                             const vid_t* __restrict__ col, vid_t u,
                                             uint32_t* R, int* DG, uint32_t* tri,
-                                            acc_t& elems) {
+                                            acc_t& elems, const eid_t* srow = nullptr) {
   const int lane = threadIdx.x & 31;
   const int gl = lane & (G - 1);
   eid_t base = 0;
@@ -153,8 +174,8 @@ __device__ __forceinline__ acc_t group_root(const eid_t* __restrict__ rowptr,
     }
   }
   __syncwarp();
-  acc_t cnt = 0;
-  if (!PAIRS && gl < d) cnt = SmallCount<K - 3, STATS>::run(R[gl], R, DG, elems);
+  acc_t cnt = 0, tt = 0;
+  if ((!PAIRS || TT) && gl < d) cnt = SmallCount<K - 3, STATS>::run(R[gl], R, DG, elems);
   if (ETRI && gl < d) {
     // the root's own arc (u, L[gl]) lies on popc(R_gl) + (rows with bit gl) triangles
     const unsigned tu = (unsigned)__popc(R[gl]) + (unsigned)DG[gl];
@@ -162,8 +183,14 @@ __device__ __forceinline__ acc_t group_root(const eid_t* __restrict__ rowptr,
       const unsigned o = atomicAdd(tri + base + gl, tu);
       if (PAIRS) pairs += pair_gain(o, tu);
     }
+    // L[gl] is the middle vertex of popc(R_gl) of the root's triangles and the top of DG[gl]
+    if (TT && tu) {
+      const acc_t dg = tt_deg(srow, Lj);
+      tt = (acc_t)__popc(R[gl]) * (tt_deg(srow, u) + dg) + (acc_t)DG[gl] * dg;
+    }
   }
   __syncwarp();
+  if (TT) return 12ull * cnt - 4ull * pairs + tt;
   return PAIRS ? pairs : cnt;
 }
 
@@ -191,13 +218,16 @@ struct DistCount {
       for (int q = 0; q < WPL; ++q) c += __popc(mw[q]);
       pm = __reduce_add_sync(kFull, (unsigned)c);
     }
-#pragma unroll
+    // one recursive call site per level (a rolled loop over the lane's words, picked from
+    // registers), so the code does not grow as WPL^depth
+#pragma unroll 1
     for (int q = 0; q < WPL; ++q) {
-      unsigned nz = __ballot_sync(kFull, mw[q] != 0u);
+      const uint32_t mq = pick_word<WPL>(mw, q);
+      unsigned nz = __ballot_sync(kFull, mq != 0u);
       while (nz) {
         const int lw = __ffs(nz) - 1;
         nz &= nz - 1;
-        uint32_t word = __shfl_sync(kFull, mw[q], lw);
+        uint32_t word = __shfl_sync(kFull, mq, lw);
         while (word) {
           const int b = __ffs(word) - 1;
           word &= word - 1;
@@ -233,13 +263,6 @@ struct DistCount<0, WPL, STATS, GR> {
 // one thread owns one first-level row and walks the deeper levels itself.  Each level has a
 // single recursive call site (code size stays linear in the depth); words are picked out of
 // the register array with an unrolled select so the masks never go to local memory.
-template <int WMAX>
-__device__ __forceinline__ uint32_t pick_word(const uint32_t (&m)[WMAX], int w) {
-  uint32_t r = 0u;
-#pragma unroll
-  for (int q = 0; q < WMAX; ++q) r = (q == w) ? m[q] : r;
-  return r;
-}
 
 template <int D, int WMAX, bool STATS>
 struct RowCount {
@@ -296,10 +319,11 @@ struct WarpSmem {
   int colcnt[kWarpMaxDeg];  // edge-triangle mode: rows with bit j set
 };
 
-template <int K, bool STATS, bool ETRI, bool PAIRS = false>
+template <int K, bool STATS, bool ETRI, bool PAIRS = false, bool TT = false>
 __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
                                            const vid_t* __restrict__ col, vid_t u, WarpSmem& ws,
-                                           uint32_t* tri, acc_t& elems) {
+                                           uint32_t* tri, acc_t& elems,
+                                           const eid_t* srow = nullptr) {
   const int lane = threadIdx.x & 31;
   const eid_t base = rowptr[u];
   const int d = (int)(rowptr[u + 1] - base);
@@ -346,7 +370,7 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
     __syncwarp();
   }
   const int T = ws.off[d];
-  acc_t pairs = 0;
+  acc_t pairs = 0, tt = 0;
   const int topL = top_pow2(d), topO = top_pow2(d - 1);
   auto hit = [&](int i, int p, vid_t x, eid_t e) {
     if (p < d && ws.L[p] == x) {
@@ -418,18 +442,24 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
     uint32_t m[kWarpW];
 #pragma unroll
     for (int q = 0; q < kWarpW; ++q) m[q] = q < w_d ? ws.R[i * w_d + q] : 0u;
-    if (!PAIRS) cnt += RowCount<K - 3, kWarpW, STATS>::run(m, ws.R, w_d, ws.deg, elems);
+    if (!PAIRS || TT) cnt += RowCount<K - 3, kWarpW, STATS>::run(m, ws.R, w_d, ws.deg, elems);
     if (ETRI) {
-      unsigned tu = (unsigned)ws.colcnt[i];
+      unsigned pc = 0;
 #pragma unroll
-      for (int q = 0; q < kWarpW; ++q) tu += (unsigned)__popc(m[q]);
+      for (int q = 0; q < kWarpW; ++q) pc += (unsigned)__popc(m[q]);
+      const unsigned tu = pc + (unsigned)ws.colcnt[i];
       if (tu) {
         const unsigned o = atomicAdd(tri + base + i, tu);
         if (PAIRS) pairs += pair_gain(o, tu);
+        if (TT) {
+          const acc_t di = tt_deg(srow, ws.L[i]);
+          tt += (acc_t)pc * (tt_deg(srow, u) + di) + (acc_t)ws.colcnt[i] * di;
+        }
       }
     }
   }
   __syncwarp();
+  if (TT) return 12ull * cnt - 4ull * pairs + tt;
   return PAIRS ? pairs : cnt;
 }
 
@@ -483,10 +513,11 @@ constexpr int kCtaRowWords = 16;
 // counted row-parallel from registers, wider ones (or all, with ROWW = 0) warp-cooperatively
 // with WPL mask words per lane (rows of up to 32 WPL words).
 template <int K, bool STATS, bool ETRI, bool PAIRS = false, int ROWW = kCtaRowWords,
-          int WPL = 1, bool GR = false>
+          int WPL = 1, bool GR = false, bool TT = false>
 __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
                                           const vid_t* __restrict__ col, vid_t u,
-                                          const MidSmem& sm, uint32_t* tri, acc_t& elems) {
+                                          const MidSmem& sm, uint32_t* tri, acc_t& elems,
+                                          const eid_t* srow = nullptr) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
@@ -545,7 +576,7 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
     __syncthreads();
   }
   const int T = off[d];
-  acc_t pairs = 0;
+  acc_t pairs = 0, tt = 0;
   const int topL = top_pow2(d), topO = top_pow2(d - 1);
   auto hit = [&](int i, int p, vid_t x, eid_t e) {
     if (p < d && L[p] == x) {
@@ -574,15 +605,20 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
   __syncthreads();
   if (ETRI) {  // the root's own arcs: popc(R_i) + (rows with bit i) triangles each
     for (int i = tid; i < d; i += nthreads) {
-      unsigned tu = (unsigned)deg[i];
-      for (int q = 0; q < w_d; ++q) tu += (unsigned)__popc(ld_row<GR>(R + (size_t)i * w_d + q));
+      unsigned pc = 0;
+      for (int q = 0; q < w_d; ++q) pc += (unsigned)__popc(ld_row<GR>(R + (size_t)i * w_d + q));
+      const unsigned tu = pc + (unsigned)deg[i];
       if (tu) {
         const unsigned o = atomicAdd(tri + base + i, tu);
         if (PAIRS) pairs += pair_gain(o, tu);
+        if (TT) {
+          const acc_t di = tt_deg(srow, L[i]);
+          tt += (acc_t)pc * (tt_deg(srow, u) + di) + (acc_t)deg[i] * di;
+        }
       }
     }
   }
-  if (PAIRS) {
+  if (PAIRS && !TT) {
     __syncthreads();
     return pairs;
   }
@@ -657,6 +693,7 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
     }
   }
   __syncthreads();
+  if (TT) return 12ull * cnt - 4ull * pairs + tt;
   return cnt;
 }
 

@@ -1,0 +1,12 @@
+// Instantiates the k-clique tier kernels for k = 6: counts and accounting (see clique_tiers.cuh).
+#include "clique_tiers.cuh"
+
+namespace jgpm {
+
+int launch_tiers_k6(int mode, const CliqueArgs& a, const TierPlan& p, int sms, cudaStream_t s,
+                    int max_out) {
+  return mode == 1 ? launch_plan_k<6, true, false>(a, p, sms, s, max_out)
+                   : launch_plan_k<6, false, false>(a, p, sms, s, max_out);
+}
+
+}  // namespace jgpm

@@ -422,6 +422,23 @@ int ensure_dag(jgpm_graph* g) {
   return JGPM_OK;
 }
 
+// out[x] for x = 0..33, then thresholds 64, 128, 256, 512, 1024, 2048, 4096: the first index
+// of the descending keys[0..n) whose key is <= the threshold.
+__global__ void k_tier_bounds(const uint32_t* keys, int32_t n, int64_t* out) {
+  const int t = threadIdx.x;
+  if (t >= 41) return;
+  const uint32_t big[7] = {64u, 128u, 256u, 512u, (uint32_t)kMidMaxDeg, 2048u,
+                           (uint32_t)kWideMaxDeg};
+  const uint32_t x = t < 34 ? (uint32_t)t : big[t - 34];
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (keys[mid] > x) lo = mid + 1;
+    else hi = mid;
+  }
+  out[t] = lo;
+}
+
 int ensure_tiers(jgpm_graph* g, int min_deg) {
   int rc;
   if ((rc = ensure_dag(g))) return rc;
@@ -451,46 +468,30 @@ int ensure_tiers(jgpm_graph* g, int min_deg) {
   JGPM_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(
       tmp.p, tb, (uint32_t*)k0.p, (uint32_t*)k1.p, g->tiers.d_roots, (int32_t*)v1.p, n, 0, 32,
       s));
-  // keys descending: [>kMidMaxDeg][33..kMidMaxDeg][min_deg..32][0...]
-  std::vector<uint32_t> hk(n);
-  JGPM_CUDA_TRY(cudaMemcpyAsync(hk.data(), k1.p, (size_t)n * sizeof(uint32_t),
-                                cudaMemcpyDeviceToHost, s));
+  // keys descending: [>kMidMaxDeg][33..kMidMaxDeg][min_deg..32][0...].  The tier boundaries
+  // (first index with key <= x for each threshold x) are found on the device; only they come
+  // back to the host.
   JGPM_CUDA_TRY(cudaMemcpyAsync(g->tiers.d_roots, v1.p, (size_t)n * sizeof(int32_t),
                                 cudaMemcpyDeviceToDevice, s));
+  constexpr int kNThr = 34 + 7;  // 0..33, then 64, 128, 256, 512, 1024, 2048, 4096
+  DevBuf bnd;
+  if ((rc = dalloc((int64_t**)&bnd.p, kNThr))) return rc;
+  k_tier_bounds<<<1, 64, 0, s>>>((const uint32_t*)k1.p, n, (int64_t*)bnd.p);
+  JGPM_CUDA_TRY(cudaGetLastError());
+  int64_t hb[kNThr];
+  JGPM_CUDA_TRY(cudaMemcpyAsync(hb, bnd.p, sizeof(hb), cudaMemcpyDeviceToHost, s));
   JGPM_CUDA_TRY(cudaStreamSynchronize(s));
-  int64_t n_large = 0, n_mid = 0, n_small = 0, n_wide_plus = 0;
-  for (int32_t i = 0; i < n; ++i) {
-    uint32_t d = hk[i];
-    if (d == 0) break;
-    if (d > (uint32_t)kWideMaxDeg) ++n_wide_plus;
-    if (d > (uint32_t)kMidMaxDeg) ++n_large;
-    else if (d > 32u) ++n_mid;
-    else ++n_small;
-  }
-  g->tiers.large_end = n_large;
-  g->tiers.wide_begin = n_wide_plus;
-  g->tiers.mid_end = n_large + n_mid;
-  g->tiers.small_end = n_large + n_mid + n_small;
-  // deg_begin[x]: first index with out-degree <= x (keys are sorted descending)
-  for (int x = 0; x < 34; ++x) {
-    int64_t lo = 0, hi = g->tiers.small_end;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi) >> 1;
-      if (hk[mid] > (uint32_t)x) lo = mid + 1;
-      else hi = mid;
-    }
-    g->tiers.deg_begin[x] = lo;
-  }
-  const uint32_t le_thr[6] = {32u, 64u, 128u, 256u, 512u, 2048u};
-  for (int q = 0; q < 6; ++q) {
-    int64_t lo = 0, hi = g->tiers.small_end;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi) >> 1;
-      if (hk[mid] > le_thr[q]) lo = mid + 1;
-      else hi = mid;
-    }
-    g->tiers.le_begin[q] = lo;
-  }
+  for (int x = 0; x < 34; ++x) g->tiers.deg_begin[x] = hb[x];
+  g->tiers.small_end = hb[0];
+  g->tiers.mid_end = hb[32];
+  g->tiers.large_end = hb[34 + 4];   // d <= kMidMaxDeg
+  g->tiers.wide_begin = hb[34 + 6];  // d <= kWideMaxDeg
+  g->tiers.le_begin[0] = hb[32];
+  g->tiers.le_begin[1] = hb[34 + 0];
+  g->tiers.le_begin[2] = hb[34 + 1];
+  g->tiers.le_begin[3] = hb[34 + 2];
+  g->tiers.le_begin[4] = hb[34 + 3];
+  g->tiers.le_begin[5] = hb[34 + 5];
   g->tiers.min_deg = min_deg;
   return JGPM_OK;
 }
@@ -729,6 +730,7 @@ int evict_graph(jgpm_graph* g, std::vector<int64_t>& h_rowptr, std::vector<int32
   g->c4_nsmall = -1;
   g->c4_nmid = 0;
   g->c4_nlarge = 0;
+  g->c4_large_keys.clear();
   g->d_rowptr = nullptr;
   g->d_col = nullptr;
   g->d_dag_rowptr = nullptr;

@@ -37,6 +37,7 @@ int launch_clique(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64_t 
                   cudaStream_t s);
 int launch_edge_triangles(jgpm_graph* g, uint32_t* d_tri, cudaStream_t s);
 int launch_diamond_pairs(jgpm_graph* g, uint32_t* d_tri, cudaStream_t s);
+int launch_induced_tt(jgpm_graph* g, uint32_t* d_tri, cudaStream_t s);
 
 enum PlanId {
   kP0 = 0, kP1 = 1, kP2 = 2, kP3 = 3, kP4 = 4, kP5 = 5, kP6 = 6, kP7 = 7, kP8 = 8, kP9 = 9,
@@ -710,6 +711,26 @@ int run_diamond_pairs(jgpm_graph* g, uint64_t* out, double* ms) {
   return JGPM_OK;
 }
 
+// Vertex-induced tailed-triangle count in one pass of the k = 4 bitmap tiers:
+// I(TT) = N(TT) - 4 N(diamond) + 12 K4 (from N(TT) = I(TT) + 4 I(D) + 12 I(K4) and
+// N(D) = I(D) + 6 I(K4)), with N(D) from the pair gains and N(TT) from the degrees of every
+// triangle's vertices.  Per-arc counters live in g->d_aux.
+int run_induced_tt(jgpm_graph* g, uint64_t* out, double* ms) {
+  int rc;
+  if ((rc = ensure_dag(g))) return rc;
+  const size_t bytes = (size_t)std::max<int64_t>(1, g->m_dag) * sizeof(uint32_t);
+  if ((rc = ensure_aux(g, bytes))) return rc;
+  Timer t;
+  cudaEventRecord(t.a, g->stream);
+  JGPM_CUDA_TRY(cudaMemsetAsync(g->d_aux, 0, bytes, g->stream));
+  if ((rc = launch_induced_tt(g, (uint32_t*)g->d_aux, g->stream))) return rc;
+  cudaEventRecord(t.b, g->stream);
+  if ((rc = read_ctl(g))) return rc;
+  *out = g->h_ctl->count[0];
+  if (ms) *ms = t.ms();
+  return JGPM_OK;
+}
+
 // Edge-induced pieces of the 4-vertex census.
 struct Census {
   unsigned __int128 sum_te, sum_c2, sum_tt, sum_path, sum_star;
@@ -830,6 +851,9 @@ int count_plan_impl(jgpm_graph* g, int id, int chunk_size, unsigned flags, bool 
     *method = JGPM_METHOD_WEDGE;
   } else if (id == kP2 && !force_plan) {
     if ((rc = run_diamond_pairs(g, &cnt, &t))) return rc;
+    *method = JGPM_METHOD_EDGE_TRIANGLE;
+  } else if (id == kITailed && !force_enum) {
+    if ((rc = run_induced_tt(g, &cnt, &t))) return rc;
     *method = JGPM_METHOD_EDGE_TRIANGLE;
   } else if (id >= kIC4 && id <= kIStar3 && !force_enum) {
     uint64_t v[6];

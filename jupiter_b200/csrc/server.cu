@@ -7,7 +7,11 @@
 // arrived while others run overlap on the device.  Admission: a query's graph must be
 // resident (the pool uploads it again, evicting least-recently-used idle graphs, if needed)
 // and the resident graph bytes plus the estimated frontier memory of everything in flight
-// must stay within the budget.  A batch's frontier is the sum of its queries' own scratch
+// must stay within the budget.  Queries on heavy graphs (more than kHeavyArcs DAG arcs) and
+// patterns the batched kernel does not cover go to kPlainWorkers plain lanes, one jgpm_count
+// each: on large graphs the per-tier plain kernels use the GPU better than the one-size batch
+// kernel, while batches win on the many small queries.  A graph is used by one batch or one
+// plain query at a time.  A batch's frontier is the sum of its queries' own scratch
 // (diamond per-arc counters) plus the largest shared scratch any of them needs (4-cycle
 // counter arena, edge-rooted list scratch), since the batch shares one context.  Counts are those of the batched kernel, i.e. exact and
 // identical to the plain per-query path.
@@ -33,6 +37,9 @@ namespace jgpm {
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+constexpr int kPlainWorkers = 2;
+constexpr int64_t kHeavyArcs = (int64_t)16 << 20;  // DAG arcs (symmetric arcs / 2)
 
 double now_s() {
   return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
@@ -60,6 +67,7 @@ struct PoolGraph {
   uint64_t bytes = 0;             // device bytes when resident
   uint64_t last_use = 0;
   int inflight = 0;
+  bool plain_busy = false;        // a plain-lane query is running on this graph
   bool resident = true;
 };
 
@@ -84,7 +92,7 @@ struct jgpm_server {
   std::deque<std::shared_ptr<jgpm::Query>> pending;
   std::deque<std::shared_ptr<jgpm::Query>> plain_pending;
   std::condition_variable cv_plain;
-  std::thread plain_thread;
+  std::vector<std::thread> plain_threads;
   std::unordered_map<uint64_t, std::shared_ptr<jgpm::Query>> tickets;
   std::vector<jgpm::PoolGraph> graphs;
   std::vector<std::unique_ptr<jgpm::Slot>> slots;
@@ -141,6 +149,10 @@ int launch_batch(jgpm_server* s, Slot& slot) {
   for (auto it = s->pending.begin(); it != s->pending.end() && (int)batch.size() < s->cfg.max_batch;) {
     std::shared_ptr<Query> q = *it;
     PoolGraph& pg = s->graphs[q->graph_id];
+    if (pg.plain_busy) {  // the graph is in a plain-lane query: next launch
+      ++it;
+      continue;
+    }
     const uint64_t with_q = own + q->fr_own + std::max(shared, q->fr_shared);
     if (!pg.resident) {
       int rc = make_resident(s, q->graph_id, with_q);
@@ -219,7 +231,10 @@ void scheduler(jgpm_server* s) {
         progress = true;
       }
     }
-    if (progress) s->cv_done.notify_all();
+    if (progress) {
+      s->cv_done.notify_all();
+      s->cv_plain.notify_all();  // graphs of completed batches are free for the plain lanes
+    }
     for (auto& sp : s->slots) {
       if (s->pending.empty()) break;
       Slot& slot = *sp;
@@ -251,7 +266,16 @@ void plain_worker(jgpm_server* s) {
       s->cv_plain.wait_for(lk, std::chrono::milliseconds(50));
       continue;
     }
-    std::shared_ptr<Query> q = s->plain_pending.front();
+    // the first pending query whose graph no batch or other plain query is using
+    auto pick = s->plain_pending.begin();
+    while (pick != s->plain_pending.end() && (s->graphs[(*pick)->graph_id].inflight > 0 ||
+                                              s->graphs[(*pick)->graph_id].plain_busy))
+      ++pick;
+    if (pick == s->plain_pending.end()) {
+      s->cv_plain.wait_for(lk, std::chrono::microseconds(200));
+      continue;
+    }
+    std::shared_ptr<Query> q = *pick;
     PoolGraph& pg = s->graphs[q->graph_id];
     if (!pg.resident) {
       int rc = make_resident(s, q->graph_id, q->frontier);
@@ -260,7 +284,7 @@ void plain_worker(jgpm_server* s) {
         continue;
       }
       if (rc) {
-        s->plain_pending.pop_front();
+        s->plain_pending.erase(pick);
         q->status = rc;
         s->cv_done.notify_all();
         continue;
@@ -270,8 +294,9 @@ void plain_worker(jgpm_server* s) {
       s->cv_plain.wait_for(lk, std::chrono::microseconds(200));
       continue;
     }
-    s->plain_pending.pop_front();
+    s->plain_pending.erase(pick);
     pg.inflight++;
+    pg.plain_busy = true;
     pg.last_use = ++s->use_clock;
     s->inflight_frontier += q->frontier;
     jgpm_graph* g = pg.g;
@@ -283,6 +308,7 @@ void plain_worker(jgpm_server* s) {
     {
       PoolGraph& pg2 = s->graphs[q->graph_id];
       pg2.inflight--;
+      pg2.plain_busy = false;
       const uint64_t b = graph_device_bytes(pg2.g);
       s->resident_bytes += b - pg2.bytes;
       pg2.bytes = b;
@@ -294,6 +320,7 @@ void plain_worker(jgpm_server* s) {
     if (rc) s->sched_error = err;
     else s->st.completed++;
     s->cv_done.notify_all();
+    s->cv_work.notify_one();  // the graph is free for batches again
   }
 }
 
@@ -319,7 +346,7 @@ void estimate_frontier(const jgpm_server* s, const jgpm_graph* g, int kind, uint
     const uint64_t cap = s->slots.empty() ? ((uint64_t)4 << 30) : s->slots[0]->ctx.c4_cap_bytes;
     *shared = 2 * std::min<uint64_t>(cap, grid * (uint64_t)g->n * 4);
   } else {
-    if (kind == kJobDiamond) *own = m_dag * 4 + 256;
+    if (kind == kJobDiamond || kind == kJobIndTT) *own = m_dag * 4 + 256;
     const int maxo = g->max_out_degree > 0 ? g->max_out_degree : g->max_degree;
     if (maxo > kBatchCtaMaxDeg) {  // wide roots: bitmap rows per CTA
       const uint64_t wd = (uint64_t)std::min(maxo, kBatchWideMaxDeg);
@@ -384,7 +411,7 @@ int jgpm_server_create(const jgpm_server_config* cfg, jgpm_server** out) {
     s->slots.push_back(std::move(sl));
   }
   s->sched = std::thread(scheduler, s);
-  s->plain_thread = std::thread(plain_worker, s);
+  for (int i = 0; i < kPlainWorkers; ++i) s->plain_threads.emplace_back(plain_worker, s);
   *out = s;
   return JGPM_OK;
 }
@@ -441,11 +468,13 @@ int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, ui
   }
   auto q = std::make_shared<Query>();
   std::string p(pattern);
-  if (p.rfind("induced:", 0) == 0) {
+  if (parse_batch_pattern(pattern, &q->kind, &q->k) == JGPM_OK) {
+    // batchable, including "induced:tailed-triangle"
+  } else if (p.rfind("induced:", 0) == 0) {
     q->plain = true;
     q->induced = 1;
     q->pattern = p.substr(8);
-  } else if (parse_batch_pattern(pattern, &q->kind, &q->k)) {
+  } else {
     q->plain = true;
     q->pattern = p;
   }
@@ -460,9 +489,20 @@ int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, ui
   }
   q->graph_id = graph_id;
   const jgpm_graph* g = s->graphs[graph_id].g;
+  if (!q->plain && g->m / 2 > kHeavyArcs) {  // heavy graph: plain lane
+    q->plain = true;
+    q->induced = p.rfind("induced:", 0) == 0 ? 1 : 0;
+    q->pattern = q->induced ? p.substr(8) : p;
+  }
   if (q->plain) {
     const uint64_t m_dag = g->m_dag > 0 ? (uint64_t)g->m_dag : (uint64_t)g->m / 2;
     q->frontier = m_dag * 4 + (uint64_t)g->n * 8 + ((uint64_t)256 << 20);
+    const std::string& qp = q->pattern;
+    if (qp == "4-cycle" || qp == "P1" || (q->induced && qp == "4-path"))
+      // the 4-cycle count's dense counters (2n ints per CTA, at most 12 GiB)
+      q->frontier += std::min<uint64_t>((uint64_t)12 << 30,
+                                        (uint64_t)device_sm_count(s->cfg.device) * 2 *
+                                            (uint64_t)g->n * 8);
   } else {
     estimate_frontier(s, g, q->kind, &q->fr_own, &q->fr_shared);
   }
@@ -593,7 +633,8 @@ int jgpm_server_destroy(jgpm_server* s) {
   s->cv_work.notify_all();
   s->cv_plain.notify_all();
   if (s->sched.joinable()) s->sched.join();
-  if (s->plain_thread.joinable()) s->plain_thread.join();
+  for (auto& t : s->plain_threads)
+    if (t.joinable()) t.join();
   for (auto& sl : s->slots) {
     if (sl->stream) cudaStreamSynchronize(sl->stream);
     if (sl->done_ev) cudaEventDestroy(sl->done_ev);

@@ -116,11 +116,13 @@ def test_replay_server_and_plain_agree(gpu, expected):
 
 
 def test_plain_lane_patterns(gpu):
-    """Non-batchable patterns (vertex-induced, reference P3..P12) run on the plain lane,
-    concurrently with batches, and give the plain counts."""
+    """Non-batchable patterns (vertex-induced diamond, reference P3..P12) run on the plain
+    lane, concurrently with batches (which also carry the batchable vertex-induced tailed
+    triangle), and give the plain counts."""
     n, ef, seed = SPECS[0]
     sym = O.rmat_graph(n, ef, 0.57, 0.19, 0.19, seed)
     want_tt = O.count("induced-tailed-triangle", sym)[0]
+    want_d = O.count("induced-diamond", sym)[0]
     want_p7 = O.count("P7", sym)[0]
     want_tri = O.count("P0", O.orient(sym))[0]
     s, ids = make_server(gpu)
@@ -128,11 +130,12 @@ def test_plain_lane_patterns(gpu):
         ts = []
         for _ in range(5):
             ts.append(("tt", s.submit(ids[0], "induced:tailed-triangle")))
+            ts.append(("d", s.submit(ids[0], "induced:diamond")))
             ts.append(("tri", s.submit(ids[0], "triangle")))
             ts.append(("p7", s.submit(ids[0], "P7")))
         for kind, t in ts:
             c, _ = s.wait(t)
-            assert c == {"tt": want_tt, "tri": want_tri, "p7": want_p7}[kind]
+            assert c == {"tt": want_tt, "d": want_d, "tri": want_tri, "p7": want_p7}[kind]
         with pytest.raises(gpu.JgpmError) as e:
             s.submit(ids[0], "induced:P7")
         assert e.value.code == -5
