@@ -483,7 +483,10 @@ def run_served(args):
         c1, lat1, w1 = srv.replay(gids, pats, arr)
         c2, lat2, w2 = srv.replay(gids, pats, arr, plain=True)
         if c1 != c2:
-            raise RuntimeError("served counts differ from the plain counts")
+            bad = [(int(g), p, int(a), int(b)) for g, p, a, b in zip(gids, pats, c1, c2) if a != b]
+            raise RuntimeError(f"served counts differ from the plain counts at {rate} q/s: "
+                               f"{len(bad)} of {nq}, e.g. (graph, pattern, served, plain) "
+                               f"{bad[:6]}")
         rows.append({"offered_qps": rate, "queries": nq,
                      "served": {"qps": nq / w1, "p50_ms": float(np.percentile(lat1, 50)),
                                 "p99_ms": float(np.percentile(lat1, 99))},

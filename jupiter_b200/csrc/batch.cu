@@ -514,7 +514,7 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   const int W = (o.dmax + 31) / 32;
   const int wW = (o.wdmax + 31) / 32;
   const size_t smem = batch_smem_bytes(o.dmax, W, o.wdmax, wW);
-  cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if ((rc = raise_smem_limit((const void*)k_batch, smem))) return rc;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, 256, smem);
   per_sm = std::max(1, std::min(per_sm, 8));

@@ -14,6 +14,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <mutex>
 
 #include "c4_dev.cuh"
 #include "jgpm_internal.h"
@@ -139,6 +140,17 @@ struct TmpBuf {
   }
 };
 
+// Counter arrays of the large apexes, cached per device when they are small (a count on a
+// small graph should not pay a cudaMalloc/cudaFree); larger ones are allocated per count so
+// that a pool of large graphs does not keep them.  The lock is held for the whole count.
+constexpr size_t kDenseCacheMax = (size_t)1 << 30;
+struct DenseCache {
+  std::mutex mu;
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+DenseCache g_dense_cache[64];
+
 }  // namespace
 
 // Classifies the apexes of g's rank CSR once: g->d_c4_small (any order) and g->d_c4_large
@@ -220,8 +232,29 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
   int64_t ctas = std::min<int64_t>((int64_t)sms * 2,
                                    ((int64_t)12 << 30) / std::max<int64_t>(1, per_cta));
   ctas = std::max<int64_t>(1, std::min<int64_t>(ctas, nlarge));
-  TmpBuf dense;
-  if (nlarge > 0 && (rc = dense.alloc((size_t)(ctas * per_cta)))) return rc;
+  const size_t dense_bytes = nlarge > 0 ? (size_t)(ctas * per_cta) : 0;
+  TmpBuf dense_tmp;
+  std::unique_lock<std::mutex> cache_lk;
+  void* dense = nullptr;
+  if (dense_bytes > 0 && dense_bytes <= kDenseCacheMax && g->device >= 0 && g->device < 64) {
+    DenseCache& dc = g_dense_cache[g->device];
+    cache_lk = std::unique_lock<std::mutex>(dc.mu);
+    if (dc.bytes < dense_bytes) {
+      if (dc.p) cudaFree(dc.p);
+      dc.p = nullptr;
+      dc.bytes = 0;
+      if (cudaMalloc(&dc.p, dense_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        jgpm_set_error_("4-cycle: device allocation failed");
+        return JGPM_ENOMEM;
+      }
+      dc.bytes = dense_bytes;
+    }
+    dense = dc.p;
+  } else if (dense_bytes > 0) {
+    if ((rc = dense_tmp.alloc(dense_bytes))) return rc;
+    dense = dense_tmp.p;
+  }
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -229,7 +262,7 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
   JGPM_CUDA_TRY(cudaMemsetAsync(g->d_ctl, 0, sizeof(DevControl), s));
   if (nsmall > 0) {
     const size_t smem = 8 * sizeof(C4WarpHash);
-    cudaFuncSetAttribute(k_c4_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if ((rc = raise_smem_limit((const void*)k_c4_small, smem))) return rc;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_small, 256, smem);
     per_sm = std::max(1, per_sm);
@@ -240,7 +273,7 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
   }
   if (nmid > 0) {
     const size_t smem = sizeof(C4CtaHash);
-    cudaFuncSetAttribute(k_c4_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if ((rc = raise_smem_limit((const void*)k_c4_mid, smem))) return rc;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_mid, 256, smem);
     per_sm = std::max(1, per_sm);
@@ -250,10 +283,10 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
     g->launches += 1;
   }
   if (nlarge > 0) {
-    JGPM_CUDA_TRY(cudaMemsetAsync(dense.p, 0, (size_t)(ctas * per_cta), s));
+    JGPM_CUDA_TRY(cudaMemsetAsync(dense, 0, dense_bytes, s));
     k_c4_large<<<(int)ctas, kC4LargeThreads, 0, s>>>(g->d_rank_rowptr, g->d_rank_col, n,
                                          g->d_c4_large, nlarge, &g->d_ctl->counter[1],
-                                         (int32_t*)dense.p, g->d_ctl);
+                                         (int32_t*)dense, g->d_ctl);
     g->launches += 1;
   }
   cudaEventRecord(e1, s);

@@ -141,6 +141,7 @@ int launch_clique_ex(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64
     case 6: n = launch_tiers_k6(mode, a, p, sms, s, mid_dmax); break;
     default: n = launch_tiers_k78(k, mode, a, p, sms, s, mid_dmax); break;
   }
+  if (n < 0) return JGPM_ECUDA;  // a tier launch failed (message set)
   g->launches += n;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

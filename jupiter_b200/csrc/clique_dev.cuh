@@ -532,7 +532,11 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
   const int d = (int)(rowptr[u + 1] - base);
   const int w_d = (d + 31) >> 5;
   for (int j = tid; j < d; j += nthreads) L[j] = __ldg(col + base + j);
-  for (int q = tid; q < d * w_d; q += nthreads) R[q] = 0u;
+  // global rows are built by L2 atomics and read at L2: clear them at L2 as well
+  for (int q = tid; q < d * w_d; q += nthreads) {
+    if (GR) __stcg(R + q, 0u);
+    else R[q] = 0u;
+  }
   __syncthreads();
   const vid_t lo_key = L[0], hi_key = L[d - 1];
   for (int i = tid; i < d; i += nthreads) {

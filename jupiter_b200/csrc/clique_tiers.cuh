@@ -253,6 +253,16 @@ __global__ void __launch_bounds__(256) k_clique_large(CliqueArgs a) {
   }
 }
 
+// True (with the error recorded) if the kernel just launched failed to launch, so that a count
+// never silently misses a tier.
+inline bool launch_failed(cudaError_t* err) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return false;
+  *err = e;
+  jgpm_set_error_(std::string("clique tier launch: ") + cudaGetErrorString(e));
+  return true;
+}
+
 // Register-mask width of a CTA band: k >= 7 counts warp-cooperatively (0), which keeps the
 // deep register-mask recursion, and its compile time, out of the large clique sizes.
 template <int K>
@@ -270,7 +280,7 @@ void launch_mid_band(CliqueArgs a, const TierRange& r, int cursor, int dmax, int
   const int W = (dmax + 31) / 32;
   const size_t sm = GR ? MidLayout{dmax, W}.bytes_no_rows() : MidLayout{dmax, W}.bytes();
   auto kern = k_clique_mid<K, STATS, ETRI, PAIRS, ROWW, WPL, GR, TT>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  raise_smem_limit((const void*)kern, sm);  // a failure shows up as the launch error
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, sm);
   if (per_sm < 1) per_sm = 1;
@@ -285,47 +295,53 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
                   int max_out) {
   CliqueArgs a = base;
   int n = 0;
+  cudaError_t err = cudaSuccess;
   if (!p.large.empty()) {
     a.begin = p.large.b;
     a.end = p.large.e;
     a.cursor = 2;
     k_clique_large<K, STATS, ETRI, PAIRS, TT><<<sms * 2, 256, 0, s>>>(a);
     ++n;
+    if (launch_failed(&err)) return -1;
   }
   if (!p.wide.empty()) {
     launch_mid_band<K, STATS, ETRI, PAIRS, 0, 4, true, TT>(a, p.wide, 9,
                                                        std::min(max_out, kWideMaxDeg), sms, s);
     ++n;
+    if (launch_failed(&err)) return -1;
   }
   if (!p.mid[0].empty()) {
     launch_mid_band<K, STATS, ETRI, PAIRS, 0, 1, false, TT>(a, p.mid[0], 1,
                                                             std::min(max_out, kMidMaxDeg),
                                               sms, s);
     ++n;
+    if (launch_failed(&err)) return -1;
   }
   if (!p.mid[1].empty()) {
     launch_mid_band<K, STATS, ETRI, PAIRS, kBandRowWords<K>(16), 1, false, TT>(a, p.mid[1], 0,
                                                                  std::min(max_out, 512), sms, s);
     ++n;
+    if (launch_failed(&err)) return -1;
   }
   if (!p.mid[2].empty()) {
     launch_mid_band<K, STATS, ETRI, PAIRS, kBandRowWords<K>(8), 1, false, TT>(a, p.mid[2], 8,
                                                                 std::min(max_out, 256), sms, s);
     ++n;
+    if (launch_failed(&err)) return -1;
   }
   if (!p.warp.empty()) {
     a.begin = p.warp.b;
     a.end = p.warp.e;
     a.cursor = 7;
     const size_t sm = 8 * sizeof(WarpSmem);
-    cudaFuncSetAttribute(k_clique_warp<K, STATS, ETRI, PAIRS, TT>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    raise_smem_limit((const void*)k_clique_warp<K, STATS, ETRI, PAIRS, TT>, sm);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clique_warp<K, STATS, ETRI, PAIRS, TT>,
                                                   256, sm);
     if (per_sm < 1) per_sm = 1;
     k_clique_warp<K, STATS, ETRI, PAIRS, TT><<<sms * per_sm, 256, sm, s>>>(a);
     ++n;
+    if (launch_failed(&err)) return -1;
   }
   const TierRange* gr[4] = {&p.g32, &p.g16, &p.g8, &p.g4};
   for (int q = 0; q < 4; ++q) {
@@ -340,6 +356,7 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
       default: k_clique_group<4, K, STATS, ETRI, PAIRS, TT><<<sms * 8, 256, 0, s>>>(a); break;
     }
     ++n;
+    if (launch_failed(&err)) return -1;
   }
   return n;
 }

@@ -8,6 +8,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -272,6 +274,24 @@ int shift_for(int32_t n) {
 }
 
 }  // namespace
+
+int raise_smem_limit(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> limits;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = limits[std::make_pair(dev, func)];
+  if (bytes <= cur) return JGPM_OK;
+  const cudaError_t e =
+      cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) {
+    jgpm_set_error_(std::string("raise_smem_limit: ") + cudaGetErrorString(e));
+    return JGPM_ECUDA;
+  }
+  cur = bytes;
+  return JGPM_OK;
+}
 
 int device_sm_count(int device) {
   int sms = 0;

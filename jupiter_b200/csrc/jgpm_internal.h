@@ -132,6 +132,10 @@ int ensure_scratch(jgpm_graph* g, size_t bytes);
 int ensure_aux(jgpm_graph* g, size_t bytes);
 void free_graph_device(jgpm_graph* g);
 int device_sm_count(int device);
+// Raises the dynamic shared-memory limit of kernel `func` on the current device to at least
+// `bytes`, never lowering it.  The limit is process-wide state and several host threads launch
+// the same kernels with different sizes, so it only grows (under a lock).
+int raise_smem_limit(const void* func, size_t bytes);
 int evict_graph(jgpm_graph* g, std::vector<int64_t>& h_rowptr, std::vector<int32_t>& h_col);
 int restore_graph(jgpm_graph* g, const std::vector<int64_t>& h_rowptr,
                   const std::vector<int32_t>& h_col);
