@@ -73,7 +73,7 @@ constexpr int kLevels = 6;
 inline size_t batch_smem_bytes(int dmax, int W, int wdmax, int wW) {
   size_t b = 8 * sizeof(WarpSmem);
   b = std::max(b, 8 * sizeof(C4WarpHash));
-  b = std::max(b, sizeof(C4CtaHash));
+  b = std::max(b, sizeof(C4MidSmem<256>));
   b = std::max(b, MidLayout{dmax, W}.bytes());
   if (wdmax > 0) b = std::max(b, MidLayout{wdmax, wW}.bytes_no_rows());
   return b;
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
   const MidSmem sm = MidSmem::carve(smem, a.dmax, a.W);
   WarpSmem& ws = reinterpret_cast<WarpSmem*>(smem)[threadIdx.x >> 5];
   C4WarpHash& hash = reinterpret_cast<C4WarpHash*>(smem)[threadIdx.x >> 5];
-  C4CtaHash& cta_hash = *reinterpret_cast<C4CtaHash*>(smem);
+  C4MidSmem<256>& c4m = *reinterpret_cast<C4MidSmem<256>*>(smem);
   __shared__ uint32_t rows[256];
   __shared__ int degs[256];
   __shared__ unsigned long long s_task;
@@ -321,10 +321,10 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
         break;
       case kTaskC4Mid:
         if (smem_kind != kTaskC4Mid) {
-          c4_cta_hash_init(cta_hash);
+          c4_cta_hash_init(c4m.h);
           smem_kind = kTaskC4Mid;
         }
-        for (int64_t q = t.b; q < t.e; ++q) c += c4_mid_apex(j.rrow, j.rcol, j.mid[q], cta_hash);
+        for (int64_t q = t.b; q < t.e; ++q) c += c4_mid_apex<256>(j.rrow, j.rcol, j.mid[q], c4m);
         break;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
@@ -333,26 +333,30 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
 }
 
 // Large 4-cycle apexes of every 4-cycle job of the batch, heaviest first, on CTAs of 1024
-// threads with one dense counter array (and touched list) of stride ints each; launched next
-// to k_batch on a second stream.
+// threads, launched next to k_batch on a second stream.  Each CTA has a shared-memory slab of
+// `words` words; an apex that needs more than kC4MaxSlices slices counts in the CTA's dense
+// array (and touched list) of `stride` ints instead when the batch has them.
 struct C4BatchArgs {
   const JobDesc* jobs;
   const Task* tasks;  // (job, apex index b)
   int64_t ntasks;
   unsigned long long* counts;
   unsigned long long* cursor;
-  int32_t* dense;
+  int32_t* dense;     // null: no apex of the batch needs one
   vid_t* touched;
   int64_t stride;
+  int words;
 };
 
 constexpr int kBatchC4Threads = 1024;
 
 __global__ void __launch_bounds__(kBatchC4Threads) k_batch_c4_large(C4BatchArgs a) {
+  extern __shared__ __align__(16) uint32_t slab[];
   __shared__ C4LargeSmem<kBatchC4Threads> sh;
   __shared__ unsigned long long s_q;
-  int32_t* dense = a.dense + (int64_t)blockIdx.x * a.stride;
-  vid_t* touched = a.touched + (int64_t)blockIdx.x * a.stride;
+  int32_t* dense = a.dense ? a.dense + (int64_t)blockIdx.x * a.stride : nullptr;
+  vid_t* touched = a.dense ? a.touched + (int64_t)blockIdx.x * a.stride : nullptr;
+  c4_slab_zero<kBatchC4Threads>(slab, a.words);  // ordered by the barriers below
   for (;;) {
     if (threadIdx.x == 0) s_q = atomicAdd(a.cursor, 1ull);
     __syncthreads();
@@ -361,7 +365,14 @@ __global__ void __launch_bounds__(kBatchC4Threads) k_batch_c4_large(C4BatchArgs 
     if (q >= a.ntasks) break;
     const Task t = a.tasks[q];
     const JobDesc j = a.jobs[t.job];
-    acc_t c = c4_large_apex(j.rrow, j.rcol, j.apexes[t.b], dense, touched, sh);
+    const vid_t v = j.apexes[t.b];
+    const eid_t b = j.rrow[v];
+    const int cut = c4_lower_bound(j.rcol + b, (int)(j.rrow[v + 1] - b), v);
+    acc_t c;
+    if (!dense || c4_slab_slices(v, cut, a.words) <= kC4MaxSlices)
+      c = c4_slab_apex<kBatchC4Threads>(j.rrow, j.rcol, v, cut, slab, a.words, sh);
+    else
+      c = c4_large_apex<kBatchC4Threads>(j.rrow, j.rcol, v, cut, dense, touched, sh);
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(&a.counts[t.job], c);
   }
@@ -390,7 +401,7 @@ int64_t tier_begin(const RootTiers& t, int x) {
 struct BuildOut {
   int dmax = 33;          // largest CTA-root out-degree
   int wdmax = 0;          // largest wide-root out-degree (0: no wide roots)
-  int64_t c4max = 0;      // largest vertex count of a job with large 4-cycle apexes
+  int64_t c4max = 0;      // largest vertex count of a job with dense-counted 4-cycle apexes
   int max_out = 0;        // largest out-degree among the large roots
   bool any_large = false;
   size_t tri_bytes = 0;   // diamond counters of the batch
@@ -426,7 +437,7 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
         c4l.push_back(Task{job, kTaskC4Large, q, q + 1});
         c4w.push_back(g->c4_large_keys[(size_t)q]);
       }
-      if (g->c4_nlarge > 0) o->c4max = std::max<int64_t>(o->c4max, g->n);
+      if (g->c4_ndense > 0) o->c4max = std::max<int64_t>(o->c4max, g->n);
       add_range_tasks(c4m, job, kTaskC4Mid, 0, g->c4_nmid, 2);
       add_range_tasks(c4s, job, kTaskC4Small, 0, g->c4_nsmall, std::max<int64_t>(8, rpt / 8));
       c.h_jobs.push_back(jd);
@@ -555,17 +566,24 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   const size_t n4 = c.h_c4_tasks.size();
   bool forked = false;
   if (n4 > 0) {
-    const size_t per_cta = (size_t)o.c4max * sizeof(int32_t);
-    const int64_t ctas = std::max<int64_t>(
-        1, std::min<int64_t>(std::min<int64_t>((int64_t)sms * 2, (int64_t)n4),
-                             (int64_t)(c.c4_cap_bytes / std::max<size_t>(1, per_cta))));
+    const size_t slab_bytes = (size_t)kC4SlabWords * sizeof(uint32_t);
+    if ((rc = raise_smem_limit((const void*)k_batch_c4_large, slab_bytes))) return rc;
+    int c4_per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c4_per_sm, k_batch_c4_large, kBatchC4Threads,
+                                                  slab_bytes);
+    int64_t ctas = std::min<int64_t>((int64_t)sms * std::max(1, c4_per_sm), (int64_t)n4);
+    const size_t per_cta = (size_t)o.c4max * sizeof(int32_t);  // 0: no dense apex
+    if (per_cta) ctas = std::min<int64_t>(ctas, (int64_t)(c.c4_cap_bytes / per_cta));
+    ctas = std::max<int64_t>(1, ctas);
     const size_t need = (size_t)ctas * per_cta;
-    if ((rc = c.c4.reserve(need))) return rc;
-    if (c.c4_zeroed < need) {  // counters are zero between apexes; zero fresh memory once
-      JGPM_CUDA_TRY(cudaMemsetAsync(c.c4.p, 0, c.c4.bytes, s));
-      c.c4_zeroed = c.c4.bytes;
+    if (need) {
+      if ((rc = c.c4.reserve(need))) return rc;
+      if (c.c4_zeroed < need) {  // counters are zero between apexes; zero fresh memory once
+        JGPM_CUDA_TRY(cudaMemsetAsync(c.c4.p, 0, c.c4.bytes, s));
+        c.c4_zeroed = c.c4.bytes;
+      }
+      if ((rc = c.c4t.reserve(need))) return rc;
     }
-    if ((rc = c.c4t.reserve(need))) return rc;
     if ((rc = c.c4_tasks.reserve(n4 * sizeof(Task)))) return rc;
     JGPM_CUDA_TRY(cudaMemcpyAsync(c.c4_tasks.p, c.h_c4_tasks.data(), n4 * sizeof(Task),
                                   cudaMemcpyHostToDevice, s));
@@ -578,10 +596,11 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     b.ntasks = (int64_t)n4;
     b.counts = (unsigned long long*)c.counts.p;
     b.cursor = (unsigned long long*)c.cursor.p + 1;
-    b.dense = (int32_t*)c.c4.p;
-    b.touched = (vid_t*)c.c4t.p;
+    b.dense = need ? (int32_t*)c.c4.p : nullptr;
+    b.touched = need ? (vid_t*)c.c4t.p : nullptr;
     b.stride = o.c4max;
-    k_batch_c4_large<<<(int)ctas, kBatchC4Threads, 0, c.side>>>(b);
+    b.words = kC4SlabWords;
+    k_batch_c4_large<<<(int)ctas, kBatchC4Threads, slab_bytes, c.side>>>(b);
     JGPM_CUDA_TRY(cudaGetLastError());
     JGPM_CUDA_TRY(cudaEventRecord(c.join_ev, c.side));
     forked = true;

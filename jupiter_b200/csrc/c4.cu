@@ -8,9 +8,11 @@
 // wedge count (sum of deg(x) over the prefix), and the classes are kept with the graph:
 //   small  (<= kC4SmallBound)  one warp per apex, counts in a shared-memory hash table;
 //   mid    (<= kC4MidBound)    one CTA per apex, counts in a CTA-wide shared-memory table;
-//   large                      one CTA per apex, counts in a dense per-CTA array in global
-//                              memory with a list of the touched vertices, heaviest apexes
-//                              first.
+//   large                      one CTA of 1024 threads per apex, heaviest apexes first, the
+//                              counts in a shared-memory slab of packed counters swept over
+//                              the vertex range in at most kC4MaxSlices slices; an apex that
+//                              needs more slices (graphs of millions of vertices) counts in a
+//                              dense per-CTA array in global memory with a touched list.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -49,6 +51,8 @@ __global__ void k_c4_classify(const eid_t* rp, const vid_t* col, vid_t n, vid_t*
         const unsigned long long p = atomicAdd(&counters[1], 1ull);
         large_list[p] = (vid_t)v;
         large_key[p] = ub;
+        if (c4_slab_slices((vid_t)v, cut, kC4SlabWords) > kC4MaxSlices)
+          atomicAdd(&counters[3], 1ull);
       }
     }
   }
@@ -73,14 +77,17 @@ __global__ void __launch_bounds__(256) k_c4_small(const eid_t* rp, const vid_t* 
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
 }
 
-__global__ void __launch_bounds__(256) k_c4_mid(const eid_t* rp, const vid_t* col,
-                                                const vid_t* list, int64_t nlist,
-                                                unsigned long long* cursor, DevControl* ctl) {
+constexpr int kC4MidThreads = 256;
+
+__global__ void __launch_bounds__(kC4MidThreads) k_c4_mid(const eid_t* rp, const vid_t* col,
+                                                          const vid_t* list, int64_t nlist,
+                                                          unsigned long long* cursor,
+                                                          DevControl* ctl) {
   extern __shared__ __align__(16) unsigned char smem[];
-  C4CtaHash& h = *reinterpret_cast<C4CtaHash*>(smem);
+  C4MidSmem<kC4MidThreads>& m = *reinterpret_cast<C4MidSmem<kC4MidThreads>*>(smem);
   __shared__ unsigned long long s_q;
   const int tid = threadIdx.x, lane = tid & 31;
-  c4_cta_hash_init(h);
+  c4_cta_hash_init(m.h);
   acc_t sum = 0;
   for (;;) {
     if (tid == 0) s_q = atomicAdd(cursor, 1ull);
@@ -88,24 +95,31 @@ __global__ void __launch_bounds__(256) k_c4_mid(const eid_t* rp, const vid_t* co
     const int64_t q = (int64_t)s_q;
     __syncthreads();
     if (q >= nlist) break;
-    sum += c4_mid_apex(rp, col, list[q], h);
+    sum += c4_mid_apex<kC4MidThreads>(rp, col, list[q], m);
   }
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
 }
 
-// 1024 threads per CTA: the dense arrays are large (n ints each), so each one is shared by as
-// many warps as a CTA holds, to keep enough atomics in flight.
+// 1024 threads per CTA: one slab (or one dense array) is shared by as many warps as a CTA
+// holds, to keep enough atomics in flight.
 constexpr int kC4LargeThreads = 1024;
 
+// Large apexes.  words > 0: each CTA has a shared-memory slab of `words` words, used by every
+// apex that needs at most kC4MaxSlices slices; the other apexes count in the CTA's dense
+// array (counters: 2n ints per CTA, n counters then n touched ids; null when no apex needs
+// one).  SLAB == false: every apex counts densely (a lighter kernel, two CTAs per SM).
+template <bool SLAB>
 __global__ void __launch_bounds__(kC4LargeThreads)
     k_c4_large(const eid_t* rp, const vid_t* col, vid_t n, const vid_t* list, int64_t nlist,
-               unsigned long long* cursor, int32_t* counters, DevControl* ctl) {
-  int32_t* dense = counters + (int64_t)blockIdx.x * 2 * n;  // n counters, then n touched ids
-  vid_t* touched = dense + n;
+               unsigned long long* cursor, int32_t* counters, int words, DevControl* ctl) {
+  extern __shared__ __align__(16) uint32_t slab[];
   __shared__ unsigned long long s_q;
   __shared__ C4LargeSmem<kC4LargeThreads> sh;
+  int32_t* dense = counters ? counters + (int64_t)blockIdx.x * 2 * n : nullptr;
+  vid_t* touched = counters ? dense + n : nullptr;
   const int tid = threadIdx.x, lane = tid & 31;
+  if (SLAB) c4_slab_zero<kC4LargeThreads>(slab, words);  // ordered by the barriers below
   acc_t sum = 0;
   for (;;) {
     if (tid == 0) s_q = atomicAdd(cursor, 1ull);
@@ -113,7 +127,15 @@ __global__ void __launch_bounds__(kC4LargeThreads)
     const int64_t q = (int64_t)s_q;
     __syncthreads();
     if (q >= nlist) break;
-    sum += c4_large_apex(rp, col, list[q], dense, touched, sh);
+    const vid_t v = list[q];
+    const eid_t b = rp[v];
+    const int cut = c4_lower_bound(col + b, (int)(rp[v + 1] - b), v);
+    // the slab is exact for any number of slices, only slower: it also takes the apexes
+    // that would rather count densely when there are no dense arrays
+    if (SLAB && (!dense || c4_slab_slices(v, cut, words) <= kC4MaxSlices))
+      sum += c4_slab_apex<kC4LargeThreads>(rp, col, v, cut, slab, words, sh);
+    else
+      sum += c4_large_apex<kC4LargeThreads>(rp, col, v, cut, dense, touched, sh);
   }
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
@@ -164,15 +186,15 @@ int ensure_c4_apexes(jgpm_graph* g) {
   TmpBuf small, mid, large, lkey, lkey2, ctr, tmp;
   if ((rc = small.alloc((size_t)n * 4)) || (rc = mid.alloc((size_t)n * 4)) ||
       (rc = large.alloc((size_t)n * 4)) || (rc = lkey.alloc((size_t)n * 8)) ||
-      (rc = ctr.alloc(3 * sizeof(unsigned long long))))
+      (rc = ctr.alloc(4 * sizeof(unsigned long long))))
     return rc;
   unsigned long long* dctr = (unsigned long long*)ctr.p;
-  JGPM_CUDA_TRY(cudaMemsetAsync(dctr, 0, 3 * sizeof(unsigned long long), s));
+  JGPM_CUDA_TRY(cudaMemsetAsync(dctr, 0, 4 * sizeof(unsigned long long), s));
   k_c4_classify<<<grid_for_c4((int64_t)n * 32), 256, 0, s>>>(
       g->d_rank_rowptr, g->d_rank_col, n, (vid_t*)small.p, (vid_t*)mid.p, (vid_t*)large.p,
       (uint64_t*)lkey.p, dctr);
   JGPM_CUDA_TRY(cudaGetLastError());
-  unsigned long long h[3] = {0, 0, 0};
+  unsigned long long h[4] = {0, 0, 0, 0};
   JGPM_CUDA_TRY(cudaMemcpyAsync(h, dctr, sizeof(h), cudaMemcpyDeviceToHost, s));
   JGPM_CUDA_TRY(cudaStreamSynchronize(s));
   const int64_t nsmall = (int64_t)h[0], nlarge = (int64_t)h[1], nmid = (int64_t)h[2];
@@ -212,6 +234,7 @@ int ensure_c4_apexes(jgpm_graph* g) {
   g->c4_nsmall = nsmall;
   g->c4_nmid = nmid;
   g->c4_nlarge = nlarge;
+  g->c4_ndense = (int64_t)h[3];
   return JGPM_OK;
 }
 
@@ -225,14 +248,30 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
   const int32_t n = g->n;
   const int sms = device_sm_count(g->device);
   const int64_t nsmall = g->c4_nsmall, nmid = g->c4_nmid, nlarge = g->c4_nlarge;
-  // dense counters and touched lists for the large apexes: 2n ints per CTA, within a 12 GiB
-  // cap.  They are allocated for this count only (a graph pool would otherwise keep one such
-  // array set per graph).
+  // Large apexes: a shared-memory slab per CTA when any apex fits one (one CTA per SM), and
+  // dense counters and touched lists (2n ints per CTA, within a 12 GiB cap) only when some
+  // apex needs more slices than allowed.  The dense arrays are allocated for this count only
+  // (a graph pool would otherwise keep one such array set per graph), or taken from a small
+  // per-device cache.
+  const int64_t ndense = g->c4_ndense;
+  const int words = nlarge > ndense ? kC4SlabWords : 0;
+  const size_t slab_bytes = (size_t)words * sizeof(uint32_t);
+  int64_t ctas = 0;
+  if (nlarge > 0) {
+    int per_sm = 2;
+    if (words > 0) {
+      if ((rc = raise_smem_limit((const void*)k_c4_large<true>, slab_bytes))) return rc;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_large<true>, kC4LargeThreads,
+                                                    slab_bytes);
+      per_sm = std::max(1, per_sm);
+    }
+    ctas = (int64_t)sms * per_sm;
+  }
   const int64_t per_cta = (int64_t)n * 8;
-  int64_t ctas = std::min<int64_t>((int64_t)sms * 2,
-                                   ((int64_t)12 << 30) / std::max<int64_t>(1, per_cta));
+  if (ndense > 0)
+    ctas = std::min<int64_t>(ctas, ((int64_t)12 << 30) / std::max<int64_t>(1, per_cta));
   ctas = std::max<int64_t>(1, std::min<int64_t>(ctas, nlarge));
-  const size_t dense_bytes = nlarge > 0 ? (size_t)(ctas * per_cta) : 0;
+  const size_t dense_bytes = ndense > 0 ? (size_t)(ctas * per_cta) : 0;
   TmpBuf dense_tmp;
   std::unique_lock<std::mutex> cache_lk;
   void* dense = nullptr;
@@ -272,21 +311,22 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
     g->launches += 1;
   }
   if (nmid > 0) {
-    const size_t smem = sizeof(C4CtaHash);
+    const size_t smem = sizeof(C4MidSmem<kC4MidThreads>);
     if ((rc = raise_smem_limit((const void*)k_c4_mid, smem))) return rc;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_mid, 256, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_mid, kC4MidThreads, smem);
     per_sm = std::max(1, per_sm);
     const int64_t grid = std::min<int64_t>((int64_t)sms * per_sm, nmid);
-    k_c4_mid<<<(int)grid, 256, smem, s>>>(g->d_rank_rowptr, g->d_rank_col, g->d_c4_mid, nmid,
+    k_c4_mid<<<(int)grid, kC4MidThreads, smem, s>>>(g->d_rank_rowptr, g->d_rank_col, g->d_c4_mid, nmid,
                                           &g->d_ctl->counter[2], g->d_ctl);
     g->launches += 1;
   }
   if (nlarge > 0) {
-    JGPM_CUDA_TRY(cudaMemsetAsync(dense, 0, dense_bytes, s));
-    k_c4_large<<<(int)ctas, kC4LargeThreads, 0, s>>>(g->d_rank_rowptr, g->d_rank_col, n,
-                                         g->d_c4_large, nlarge, &g->d_ctl->counter[1],
-                                         (int32_t*)dense, g->d_ctl);
+    if (dense_bytes) JGPM_CUDA_TRY(cudaMemsetAsync(dense, 0, dense_bytes, s));
+    auto kern = words > 0 ? k_c4_large<true> : k_c4_large<false>;
+    kern<<<(int)ctas, kC4LargeThreads, slab_bytes, s>>>(
+        g->d_rank_rowptr, g->d_rank_col, n, g->d_c4_large, nlarge, &g->d_ctl->counter[1],
+        (int32_t*)dense, words, g->d_ctl);
     g->launches += 1;
   }
   cudaEventRecord(e1, s);

@@ -10,20 +10,29 @@
 // and c(v0, v3) is the number of wedges that end at v3.  The count equals the reference's P1
 // plan (src/message_passing_gpu_kernels.cuh:104-186), which fixes each cycle at its largest
 // vertex id instead.
+//
+// Every counter add returns the count before it, and C(c, 2) = 0 + 1 + ... + (c - 1), so the
+// sum of the returned counts is sum C(c, 2): no pass reads the counters back.  The passes
+// after the adds only put the counters back to zero.
 #pragma once
 #include "jgpm_internal.h"
 #include "setops.cuh"
 
 namespace jgpm {
 
-// Apex classes by their wedge upper bound (sum of deg(x) over the prefix):
-//   small  <= kC4SmallBound  one warp, shared-memory hash of kC4HashSlots (load <= 1/2);
-//   mid    <= kC4MidBound    one CTA, shared-memory hash of kC4MidSlots (load <= 1/2);
-//   large                    one CTA, dense counter array in global memory.
+// Apex classes by their wedge upper bound ub (sum of deg(x) over the prefix):
+//   small  ub <= kC4SmallBound  one warp, shared-memory hash of kC4HashSlots (load <= 1/2);
+//   mid    ub <= kC4MidBound    one CTA, shared-memory hash of kC4MidSlots (load <= 1/2);
+//   large                       one CTA of 1024 threads, either a shared-memory slab of packed
+//                               counters swept over the vertex range in at most kC4MaxSlices
+//                               slices, or (more slices) a dense counter array in global
+//                               memory.
 constexpr int kC4SmallBound = 256;
 constexpr int kC4HashSlots = 512;
 constexpr int kC4MidBound = 2048;
 constexpr int kC4MidSlots = 4096;
+constexpr int kC4SlabWords = 48 * 1024;  // 192 KB of 32-bit words
+constexpr int kC4MaxSlices = 4;
 
 // Per-warp shared memory of the small-apex path.
 struct C4WarpHash {
@@ -34,7 +43,7 @@ struct C4WarpHash {
   int pad[3];
 };
 
-// Shared memory of the mid-apex path (one per CTA).
+// Hash table of the mid-apex path (one per CTA).
 struct C4CtaHash {
   int keys[kC4MidSlots];  // -1 = empty
   int cnt[kC4MidSlots];
@@ -43,6 +52,35 @@ struct C4CtaHash {
   int cut;
   int pad[2];
 };
+
+// Block-wide wedge layout of a CTA of up to NT threads: thread r owns the wedges
+// [off[r], off[r+1]) of the flattened range, read from col[bx[r] ..].
+template <int NT>
+struct C4LargeSmem {
+  int cut, nt;
+  int off[NT + 1];  // exclusive offsets, off[NT] = total
+  int wsum[NT / 32];
+  eid_t bx[NT];
+};
+
+// Shared memory of the mid-apex path: the table and the wedge layout.
+template <int NT>
+struct C4MidSmem {
+  C4CtaHash h;
+  C4LargeSmem<NT> f;
+};
+
+// log2 of the counter width of a slab apex with `cut` lower-ranked neighbours: every count is
+// at most cut, so 8-bit counters do for cut < 256 and 16-bit ones for cut < 65536.
+__host__ __device__ __forceinline__ int c4_slab_lgbits(int cut) {
+  return cut < 256 ? 3 : cut < 65536 ? 4 : 5;
+}
+
+// Slices of `words` 32-bit words needed to cover the vertex ids [0, v).
+__host__ __device__ __forceinline__ int64_t c4_slab_slices(vid_t v, int cut, int words) {
+  const int64_t span = (int64_t)words << (5 - c4_slab_lgbits(cut));
+  return ((int64_t)v + span - 1) / span;
+}
 
 __device__ __forceinline__ int top_pow2_c4(int n) { return n > 0 ? 1 << (31 - __clz(n)) : 0; }
 
@@ -94,29 +132,23 @@ __device__ __forceinline__ void c4_wedge_chunk(const eid_t* rp, const vid_t* col
 }
 
 // Adds one wedge ending at v3 to an open-addressing table (keys -1 = empty) whose load stays
-// at most 1/2; slots taken for the first time are appended to used[].
+// at most 1/2; slots taken for the first time are appended to used[].  Returns the count of v3
+// before this wedge.
 template <int SLOTS, int SHIFT>
-__device__ __forceinline__ void c4_hash_add(int* keys, int* cnt, int* used, int* nused,
-                                            vid_t v3) {
+__device__ __forceinline__ int c4_hash_add(int* keys, int* cnt, int* used, int* nused,
+                                           vid_t v3) {
   volatile int* vkeys = keys;
   int s = (int)(((uint32_t)v3 * 0x9E3779B1u) >> SHIFT);
   for (;;) {
     const int k = vkeys[s];
-    if (k == v3) {
-      atomicAdd(&cnt[s], 1);
-      return;
-    }
+    if (k == v3) return atomicAdd(&cnt[s], 1);
     if (k == -1) {
       const int old = atomicCAS(&keys[s], -1, v3);
       if (old == -1) {
-        atomicAdd(&cnt[s], 1);
         used[atomicAdd(nused, 1)] = s;
-        return;
+        return atomicAdd(&cnt[s], 1);
       }
-      if (old == v3) {
-        atomicAdd(&cnt[s], 1);
-        return;
-      }
+      if (old == v3) return atomicAdd(&cnt[s], 1);
     }
     s = (s + 1) & (SLOTS - 1);
   }
@@ -143,18 +175,16 @@ __device__ __forceinline__ acc_t c4_small_apex(const eid_t* rp, const vid_t* col
   int cut = 0;
   if (lane == 0) cut = c4_lower_bound(col + b, d, v);
   cut = __shfl_sync(kFull, cut, 0);
+  acc_t sum = 0;
   for (int c0 = 0; c0 < cut; c0 += 32) {
     c4_wedge_chunk(rp, col, v, b, cut, c0, [&](vid_t v3) {
-      c4_hash_add<kC4HashSlots, 23>(h.keys, h.cnt, h.used, &h.nused, v3);  // 9-bit hash
+      sum += (acc_t)c4_hash_add<kC4HashSlots, 23>(h.keys, h.cnt, h.used, &h.nused, v3);
     });
   }
   __syncwarp();
-  acc_t sum = 0;
   const int nu = h.nused;
   for (int u = lane; u < nu; u += 32) {
     const int s = h.used[u];
-    const acc_t c = (acc_t)h.cnt[s];
-    sum += c * (c - 1) / 2;
     h.keys[s] = -1;
     h.cnt[s] = 0;
   }
@@ -164,54 +194,6 @@ __device__ __forceinline__ acc_t c4_small_apex(const eid_t* rp, const vid_t* col
   return sum;
 }
 
-// Empties a CTA's mid-apex table (every thread calls it; ends with a barrier).
-__device__ __forceinline__ void c4_cta_hash_init(C4CtaHash& h) {
-  for (int q = threadIdx.x; q < kC4MidSlots; q += blockDim.x) {
-    h.keys[q] = -1;
-    h.cnt[q] = 0;
-  }
-  if (threadIdx.x == 0) h.nused = 0;
-  __syncthreads();
-}
-
-// One mid apex v (wedge bound <= kC4MidBound) on the whole CTA with the shared table (empty on
-// entry, empty again on return).  Every thread calls it.  Returns this thread's share.
-__device__ __forceinline__ acc_t c4_mid_apex(const eid_t* rp, const vid_t* col, vid_t v,
-                                             C4CtaHash& h) {
-  const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5;
-  const eid_t b = rp[v];
-  const int d = (int)(rp[v + 1] - b);
-  if (tid == 0) h.cut = c4_lower_bound(col + b, d, v);
-  __syncthreads();
-  const int cut = h.cut;
-  for (int c0 = warp * 32; c0 < cut; c0 += nw * 32)
-    c4_wedge_chunk(rp, col, v, b, cut, c0, [&](vid_t v3) {
-      c4_hash_add<kC4MidSlots, 20>(h.keys, h.cnt, h.used, &h.nused, v3);  // 12-bit hash
-    });
-  __syncthreads();
-  acc_t sum = 0;
-  const int nu = h.nused;
-  for (int u = tid; u < nu; u += blockDim.x) {
-    const int s = h.used[u];
-    const acc_t c = (acc_t)h.cnt[s];
-    sum += c * (c - 1) / 2;
-    h.keys[s] = -1;
-    h.cnt[s] = 0;
-  }
-  __syncthreads();
-  if (tid == 0) h.nused = 0;
-  __syncthreads();
-  return sum;
-}
-
-// Shared memory of the large-apex path for CTAs of up to NT threads.
-template <int NT>
-struct C4LargeSmem {
-  int cut, nt;
-  int off[NT + 1];  // exclusive offsets of the block's x wedge counts, off[NT] = total
-  int wsum[NT / 32];
-  eid_t bx[NT];     // start of prefix(N(x), v) for the block's x
-};
 
 // Binary lifting over a sorted shared-memory array (fixed trip count, top = largest power of
 // two <= n): two independent searches in lockstep, p = #{a[j] < x}.
@@ -225,28 +207,70 @@ __device__ __forceinline__ void c4_count_below2(const int* a, int n, int top, in
   }
 }
 
-// One large apex v on the whole CTA.  The lower-ranked neighbours x are taken in blocks of
-// blockDim; each block's wedges (one thread computes |prefix(N(x), v)| per x, a block scan
-// gives the offsets) are spread over all threads, two per thread and iteration, so one hub x
-// does not hold up a single warp.  Pass 0 adds every wedge to the dense array (zero on entry)
-// and appends each vertex counted for the first time to the touched list; pass 1 reads and
-// clears only the touched counters.  Every thread calls it.  Returns this thread's share of
-// sum C(c, 2).
+// Lays out the wedges of one block of lower-ranked neighbours, one per thread: `len` wedges read
+// from col[start ..].  Exclusive block scan into sh.off (sh.off[NT] = total), which it returns.
+// Every thread of the CTA (blockDim.x == NT) calls it; it ends with a barrier.  A caller that
+// reads sh after it puts a barrier before the next call.
 template <int NT>
-__device__ __forceinline__ acc_t c4_large_apex(const eid_t* rp, const vid_t* col, vid_t v,
-                                               int32_t* dense, vid_t* touched,
-                                               C4LargeSmem<NT>& sh) {
+__device__ __forceinline__ int c4_block_layout(int len, eid_t start, C4LargeSmem<NT>& sh) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nth = blockDim.x;
-  const eid_t b = rp[v];
-  const int d = (int)(rp[v + 1] - b);
-  if (tid == 0) {
-    sh.cut = c4_lower_bound(col + b, d, v);
-    sh.nt = 0;
+  int incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
   }
+  if (lane == 31) sh.wsum[warp] = incl;
   __syncthreads();
-  const int cut = sh.cut;
-  for (int base = 0; base < cut; base += nth) {
+  int wbase = 0;
+  for (int w = 0; w < warp; ++w) wbase += sh.wsum[w];
+  sh.off[tid] = wbase + incl - len;
+  sh.bx[tid] = start;
+  if (tid == NT - 1) sh.off[NT] = wbase + incl;
+  __syncthreads();
+  return sh.off[NT];
+}
+
+// Calls visit(v3) once for each of the T wedges of the layout, spread over all threads, two per
+// thread and iteration (so a hub x does not hold up one warp).  rows = number of threads that
+// own wedges (a prefix of the block).
+template <int NT, typename Visit>
+__device__ __forceinline__ void c4_flat_wedges(const vid_t* col, const C4LargeSmem<NT>& sh,
+                                               int rows, int T, Visit visit) {
+  const int top = top_pow2_c4(rows - 1);
+  for (int t0 = threadIdx.x; t0 < T; t0 += 2 * NT) {
+    const bool two = t0 + NT < T;
+    const int t1 = two ? t0 + NT : t0;
+    int r0, r1;  // owner of wedge t = last r with off[r] <= t
+    c4_count_below2(sh.off + 1, rows - 1, top, t0 + 1, t1 + 1, r0, r1);
+    const vid_t a0 = __ldg(col + sh.bx[r0] + (t0 - sh.off[r0]));
+    const vid_t a1 = __ldg(col + sh.bx[r1] + (t1 - sh.off[r1]));
+    visit(a0);
+    if (two) visit(a1);
+  }
+}
+
+// Empties a CTA's mid-apex table (every thread calls it; ends with a barrier).
+__device__ __forceinline__ void c4_cta_hash_init(C4CtaHash& h) {
+  for (int q = threadIdx.x; q < kC4MidSlots; q += blockDim.x) {
+    h.keys[q] = -1;
+    h.cnt[q] = 0;
+  }
+  if (threadIdx.x == 0) h.nused = 0;
+  __syncthreads();
+}
+
+// One mid apex v (wedge bound <= kC4MidBound) on the whole CTA (NT threads) with the shared
+// table (empty on entry, empty again on return).  The wedges are flattened over all threads.
+// Every thread calls it.  Returns this thread's share of sum C(c, 2).
+template <int NT>
+__device__ __forceinline__ acc_t c4_mid_apex(const eid_t* rp, const vid_t* col, vid_t v,
+                                             C4MidSmem<NT>& m) {
+  const int tid = threadIdx.x;
+  const eid_t b = rp[v];
+  const int cut = c4_lower_bound(col + b, (int)(rp[v + 1] - b), v);
+  acc_t sum = 0;
+  for (int base = 0; base < cut; base += NT) {
     const int i = base + tid;
     int len = 0;
     eid_t bx = 0;
@@ -255,42 +279,140 @@ __device__ __forceinline__ acc_t c4_large_apex(const eid_t* rp, const vid_t* col
       bx = rp[x];
       len = c4_lower_bound(col + bx, (int)(rp[x + 1] - bx), v);
     }
-    // block exclusive scan of len
-    int incl = len;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) sh.wsum[warp] = incl;
+    const int T = c4_block_layout<NT>(len, bx, m.f);
+    c4_flat_wedges<NT>(col, m.f, min(NT, cut - base), T, [&](vid_t v3) {
+      sum += (acc_t)c4_hash_add<kC4MidSlots, 20>(m.h.keys, m.h.cnt, m.h.used, &m.h.nused, v3);
+    });
     __syncthreads();
-    int wbase = 0;
-    for (int w = 0; w < warp; ++w) wbase += sh.wsum[w];
-    sh.off[tid] = wbase + incl - len;
-    sh.bx[tid] = bx;
-    if (tid == nth - 1) sh.off[nth] = wbase + incl;
-    __syncthreads();
-    const int T = sh.off[nth];
-    const int top = top_pow2_c4(nth - 1);
-    for (int t0 = tid; t0 < T; t0 += 2 * nth) {
-      const bool two = t0 + nth < T;
-      const int t1 = two ? t0 + nth : t0;
-      int r0, r1;  // row of element t = last r with off[r] <= t
-      c4_count_below2(sh.off + 1, nth - 1, top, t0 + 1, t1 + 1, r0, r1);
-      const vid_t v30 = __ldg(col + sh.bx[r0] + (t0 - sh.off[r0]));
-      const vid_t v31 = __ldg(col + sh.bx[r1] + (t1 - sh.off[r1]));
-      if (atomicAdd(&dense[v30], 1) == 0) touched[atomicAdd(&sh.nt, 1)] = v30;
-      if (two && atomicAdd(&dense[v31], 1) == 0) touched[atomicAdd(&sh.nt, 1)] = v31;
+  }
+  const int nu = m.h.nused;
+  for (int u = tid; u < nu; u += NT) {
+    const int s = m.h.used[u];
+    m.h.keys[s] = -1;
+    m.h.cnt[s] = 0;
+  }
+  __syncthreads();
+  if (tid == 0) m.h.nused = 0;
+  __syncthreads();
+  return sum;
+}
+
+// One large apex v with `cut` lower-ranked neighbours on the whole CTA (NT threads), counted in
+// a dense array of the CTA in global memory (zero on entry, zero again on return); the vertices
+// counted for the first time go to the touched list, which the last pass clears.  Every thread
+// calls it.  Returns this thread's share of sum C(c, 2).
+template <int NT>
+__device__ __forceinline__ acc_t c4_large_apex(const eid_t* rp, const vid_t* col, vid_t v,
+                                               int cut, int32_t* dense, vid_t* touched,
+                                               C4LargeSmem<NT>& sh) {
+  const int tid = threadIdx.x;
+  const eid_t b = rp[v];
+  if (tid == 0) sh.nt = 0;  // ordered before the adds by the layout's barriers
+  acc_t sum = 0;
+  for (int base = 0; base < cut; base += NT) {
+    const int i = base + tid;
+    int len = 0;
+    eid_t bx = 0;
+    if (i < cut) {
+      const vid_t x = __ldg(col + b + i);
+      bx = rp[x];
+      len = c4_lower_bound(col + bx, (int)(rp[x + 1] - bx), v);
     }
+    const int T = c4_block_layout<NT>(len, bx, sh);
+    c4_flat_wedges<NT>(col, sh, min(NT, cut - base), T, [&](vid_t v3) {
+      const int old = atomicAdd(&dense[v3], 1);
+      if (old == 0) touched[atomicAdd(&sh.nt, 1)] = v3;
+      sum += (acc_t)old;
+    });
     __syncthreads();
   }
   const int nt = sh.nt;
-  acc_t sum = 0;
-  for (int q = tid; q < nt; q += nth) {
-    const acc_t c = (acc_t)atomicExch(&dense[touched[q]], 0);
-    sum += c * (c - 1) / 2;
-  }
+  for (int q = tid; q < nt; q += NT) atomicExch(&dense[touched[q]], 0);
   __syncthreads();
+  return sum;
+}
+
+// Zeroes the first `words` words of a shared-memory slab (16-byte aligned; words % 4 == 0).
+template <int NT>
+__device__ __forceinline__ void c4_slab_zero(uint32_t* slab, int words) {
+  uint4* p = reinterpret_cast<uint4*>(slab);
+  for (int q = threadIdx.x; q < (words >> 2); q += NT) p[q] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// One large apex v with `cut` lower-ranked neighbours on the whole CTA (NT threads), counted in
+// a shared-memory slab of `words` words (zero on entry, zero again on return).  The counters are
+// packed 32 / 2^lgb to a word (c4_slab_lgbits: no count overflows its field), and the endpoint
+// range [0, v) is swept in slices of words * 32 / 2^lgb ids.  Each prefix(N(x), v) is sorted, so
+// one binary search per (x, slice) gives the wedges of the slice and no wedge is read twice.
+// Every thread calls it.  Returns this thread's share of sum C(c, 2).
+template <int NT>
+__device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col, vid_t v,
+                                              int cut, uint32_t* slab, int words,
+                                              C4LargeSmem<NT>& sh) {
+  const int tid = threadIdx.x;
+  const eid_t b = rp[v];
+  const int lgb = c4_slab_lgbits(cut);
+  const int lgper = 5 - lgb;                // log2 of counters per word
+  const uint32_t lmask = (1u << lgper) - 1u;
+  const uint32_t cmask = lgb == 5 ? 0xffffffffu : (1u << (1 << lgb)) - 1u;
+  const int64_t span = (int64_t)words << lgper;
+  const int nblk = (cut + NT - 1) / NT;
+  // one block of x: this thread's x list and its cursor, kept across the slices
+  eid_t xb = 0;
+  int xd = 0, cur = 0;
+  if (nblk == 1 && tid < cut) {
+    const vid_t x = __ldg(col + b + tid);
+    xb = rp[x];
+    xd = (int)(rp[x + 1] - xb);
+  }
+  acc_t sum = 0;
+  for (int64_t lo = 0; lo < (int64_t)v; lo += span) {
+    const vid_t lo32 = (vid_t)lo;
+    const vid_t hi = (vid_t)(lo + span < (int64_t)v ? lo + span : (int64_t)v);
+    int added = 0;
+    for (int blk = 0; blk < nblk; ++blk) {
+      const int i = blk * NT + tid;
+      int len = 0;
+      eid_t start = 0;
+      if (i < cut) {
+        if (nblk == 1) {
+          const int e = cur + c4_lower_bound(col + xb + cur, xd - cur, hi);
+          start = xb + cur;
+          len = e - cur;
+          cur = e;
+        } else {
+          const vid_t x = __ldg(col + b + i);
+          const eid_t bx = rp[x];
+          const int dx = (int)(rp[x + 1] - bx);
+          const int s0 = lo32 == 0 ? 0 : c4_lower_bound(col + bx, dx, lo32);
+          start = bx + s0;
+          len = c4_lower_bound(col + start, dx - s0, hi);
+        }
+      }
+      const int T = c4_block_layout<NT>(len, start, sh);
+      if (T > 0) {
+        c4_flat_wedges<NT>(col, sh, min(NT, cut - blk * NT), T, [&](vid_t v3) {
+          const uint32_t l = (uint32_t)(v3 - lo32);
+          const int sft = (int)(l & lmask) << lgb;
+          const uint32_t old = atomicAdd(slab + (l >> lgper), 1u << sft);
+          sum += (acc_t)((old >> sft) & cmask);
+        });
+        __syncthreads();
+      }
+      added += T;
+    }
+    if (added > 0) {
+      if (nblk == 1 && added <= (words >> 4)) {
+        // few wedges: zero the words they touched (the layout of the one block is still in sh)
+        c4_flat_wedges<NT>(col, sh, min(NT, cut), added, [&](vid_t v3) {
+          slab[(uint32_t)(v3 - lo32) >> lgper] = 0u;
+        });
+      } else {
+        c4_slab_zero<NT>(slab, ((int)(((uint32_t)(hi - lo32) + lmask) >> lgper) + 3) & ~3);
+      }
+      __syncthreads();
+    }
+  }
   return sum;
 }
 

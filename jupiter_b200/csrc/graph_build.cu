@@ -750,6 +750,7 @@ int evict_graph(jgpm_graph* g, std::vector<int64_t>& h_rowptr, std::vector<int32
   g->c4_nsmall = -1;
   g->c4_nmid = 0;
   g->c4_nlarge = 0;
+  g->c4_ndense = 0;
   g->c4_large_keys.clear();
   g->d_rowptr = nullptr;
   g->d_col = nullptr;

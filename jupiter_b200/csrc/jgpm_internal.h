@@ -78,13 +78,14 @@ struct jgpm_graph {
   int64_t* d_rank_rowptr = nullptr;
   int32_t* d_rank_col = nullptr;
   // 4-cycle apexes of the rank CSR by wedge bound (built on demand): one-warp, one-CTA
-  // shared-memory and dense-counter classes, the last sorted by descending bound
+  // hash and large (slab or dense counter) classes, the last sorted by descending bound
   int32_t* d_c4_small = nullptr;
   int32_t* d_c4_mid = nullptr;
   int32_t* d_c4_large = nullptr;
   int64_t c4_nsmall = -1;  // -1 = not built
   int64_t c4_nmid = 0;
   int64_t c4_nlarge = 0;
+  int64_t c4_ndense = 0;   // large apexes that need more slab slices than allowed
   std::vector<uint64_t> c4_large_keys;  // host copy: wedge bound of each large apex, descending
   int32_t max_out_degree = 0;
   jgpm::RootTiers tiers;

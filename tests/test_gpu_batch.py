@@ -129,6 +129,29 @@ def test_batch_large_roots_complete_graph(gpu, mixed):
                 assert c == want[(gs.index(g), p)], (gs.index(g), p)
 
 
+def test_batch_c4_slab_and_dense(gpu, mixed):
+    """Large 4-cycle apexes in the batch's side kernel: slabs over several slices with 8-, 16-
+    and 32-bit counters, and dense arrays for the apexes past the slice cap, next to small
+    graphs.  Against the oracle and the K_{2,N} closed form."""
+    from math import comb
+    from test_gpu_parity import bipartite_2n, c4_slab_graphs
+    specs, gs, want = mixed
+    N = 70000
+    big = [gpu.Graph.rmat(*spec) for spec in c4_slab_graphs()]
+    try:
+        with bipartite_2n(gpu, N) as kb:
+            jobs = [(g, "4-cycle") for g in big] + [(kb, "4-cycle")] + \
+                [(g, "4-cycle") for g in gs[:4]]
+            exp = [O.count("P1", O.rmat_graph(*spec))[0] for spec in c4_slab_graphs()] + \
+                [comb(N, 2)] + [want[(i, "4-cycle")] for i in range(4)]
+            counts, st = gpu.batch_count(jobs)
+            assert counts == exp
+            assert st["launches"] == 2
+    finally:
+        for g in big:
+            g.close()
+
+
 def test_batch_list_roots_crown(gpu, mixed):
     """Roots of out-degree 5000 (above the batched bitmap limits) run on edge-rooted lists in
     the batch: the crown graph of test_gpu_parity (closed forms), batched with small graphs."""

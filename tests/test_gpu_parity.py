@@ -191,6 +191,36 @@ def test_large_roots_against_oracle(gpu):
         assert g.count("diamond") == g.count("P2", flags=gpu.COUNT_FORCE_PLAN)
 
 
+def c4_slab_graphs():
+    """R-MAT graphs whose large 4-cycle apexes cover the slab forms: 2^18 vertices (two and
+    three slices, 8- and 16-bit counters) and 2^20 (the top-ranked apexes past the slice cap,
+    in dense arrays)."""
+    return [(1 << 18, 8, 0.6, 0.1, 0.1, 11), (1 << 20, 4, 0.6, 0.1, 0.1, 11)]
+
+
+def bipartite_2n(J, N):
+    """K_{2,N}: hubs 0 and 1 joined to the leaves 2 .. N+1."""
+    leaves = np.arange(2, N + 2, dtype=np.int32)
+    s = np.concatenate([np.zeros(N, np.int32), np.ones(N, np.int32)])
+    return J.Graph.from_edges(s, np.concatenate([leaves, leaves]), N + 2)
+
+
+def test_c4_slab_slices_and_dense_apexes(gpu):
+    for spec in c4_slab_graphs():
+        sym = O.rmat_graph(*spec)
+        with gpu.Graph.rmat(*spec) as g:
+            assert g.count("4-cycle") == O.count("P1", sym)[0], spec
+
+
+def test_c4_slab_wide_counters(gpu):
+    """K_{2,N} with N = 70000: the top hub has N lower-ranked neighbours (32-bit counters,
+    69 blocks of 1024 neighbours, two slices, every wedge in the second).  C4 = C(N, 2)."""
+    from math import comb
+    N = 70000
+    with bipartite_2n(gpu, N) as g:
+        assert g.count("4-cycle") == comb(N, 2)
+
+
 @pytest.mark.parametrize("pattern", ["triangle", "4-clique", "5-clique", "P1", "P2", "P7"])
 def test_rounds_do_not_change_counts(gpu, graphs, pattern):
     g = graphs["rmat-n4096-ef8-s5"]
