@@ -366,8 +366,7 @@ __global__ void __launch_bounds__(kBatchC4Threads) k_batch_c4_large(C4BatchArgs 
     const Task t = a.tasks[q];
     const JobDesc j = a.jobs[t.job];
     const vid_t v = j.apexes[t.b];
-    const eid_t b = j.rrow[v];
-    const int cut = c4_lower_bound(j.rcol + b, (int)(j.rrow[v + 1] - b), v);
+    const int cut = j.apexes[j.nlarge + t.b];
     acc_t c;
     if (!dense || c4_slab_slices(v, cut, a.words) <= kC4MaxSlices)
       c = c4_slab_apex<kBatchC4Threads>(j.rrow, j.rcol, v, cut, slab, a.words, sh);
@@ -432,6 +431,7 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
       jd.rcol = g->d_rank_col;
       jd.roots = g->d_c4_small;
       jd.apexes = g->d_c4_large;
+      jd.nlarge = (int32_t)g->c4_nlarge;
       jd.mid = g->d_c4_mid;
       for (int64_t q = 0; q < g->c4_nlarge; ++q) {
         c4l.push_back(Task{job, kTaskC4Large, q, q + 1});
@@ -492,16 +492,17 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
     }
     c.h_jobs.push_back(jd);
   }
-  // large 4-cycle apexes (all jobs', by descending wedge bound) go to k_batch_c4_large; the
-  // main queue: large roots, CTA roots, mid apexes, warp roots, small apexes, lane groups
+  // large 4-cycle apexes go to k_batch_c4_large job by job (so that the CTAs share one or two
+  // graphs in L2 at a time), jobs by descending total wedge bound, each job's apexes by
+  // descending bound (their order in the graph's list); the main queue: large roots, CTA
+  // roots, mid apexes, warp roots, small apexes, lane groups
   if (c4l.size() > 1) {
-    std::vector<uint32_t> ord(c4l.size());
-    for (size_t q = 0; q < ord.size(); ++q) ord[q] = (uint32_t)q;
-    std::stable_sort(ord.begin(), ord.end(),
-                     [&](uint32_t x, uint32_t y) { return c4w[x] > c4w[y]; });
-    std::vector<Task> sorted(c4l.size());
-    for (size_t q = 0; q < ord.size(); ++q) sorted[q] = c4l[ord[q]];
-    c4l.swap(sorted);
+    std::vector<uint64_t> weight(c.h_jobs.size(), 0);
+    for (size_t q = 0; q < c4l.size(); ++q) weight[(size_t)c4l[q].job] += c4w[q];
+    std::stable_sort(c4l.begin(), c4l.end(), [&](const Task& x, const Task& y) {
+      const uint64_t wx = weight[(size_t)x.job], wy = weight[(size_t)y.job];
+      return wx != wy ? wx > wy : x.job < y.job;
+    });
   }
   c.h_c4_tasks.swap(c4l);
   c.h_tasks.reserve(heavy.size() + cta.size() + c4m.size() + warp.size() + c4s.size() +

@@ -44,14 +44,14 @@ struct JobDesc {
   const eid_t* rrow;    // rank-relabelled symmetric CSR (4-cycle)
   const vid_t* rcol;
   const vid_t* roots;   // root tiers (descending out-degree), or the small 4-cycle apexes
-  const vid_t* apexes;  // large 4-cycle apexes (descending wedge bound)
+  const vid_t* apexes;  // large 4-cycle apexes (descending wedge bound), then their cuts
   const vid_t* mid;     // mid 4-cycle apexes
   uint32_t* tri;        // diamond, tailed triangle: per-arc triangle counters (zero at launch)
   const eid_t* srow;    // tailed triangle: symmetric row pointers (degrees)
   int32_t n;
   int32_t kind;
   int32_t k;
-  int32_t pad;
+  int32_t nlarge;       // large 4-cycle apexes
 };
 
 struct Task {

@@ -77,6 +77,17 @@ __global__ void __launch_bounds__(256) k_c4_small(const eid_t* rp, const vid_t* 
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
 }
 
+// Lower-ranked neighbour count (the cut) of each large apex, stored after the apex list.
+__global__ void k_c4_cuts(const eid_t* rp, const vid_t* col, const vid_t* list, int64_t nlist,
+                          int32_t* cuts) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nlist; q += stride) {
+    const vid_t v = list[q];
+    const eid_t b = rp[v];
+    cuts[q] = c4_lower_bound(col + b, (int)(rp[v + 1] - b), v);
+  }
+}
+
 constexpr int kC4MidThreads = 256;
 
 __global__ void __launch_bounds__(kC4MidThreads) k_c4_mid(const eid_t* rp, const vid_t* col,
@@ -113,6 +124,7 @@ template <bool SLAB>
 __global__ void __launch_bounds__(kC4LargeThreads)
     k_c4_large(const eid_t* rp, const vid_t* col, vid_t n, const vid_t* list, int64_t nlist,
                unsigned long long* cursor, int32_t* counters, int words, DevControl* ctl) {
+  const int32_t* cuts = list + nlist;
   extern __shared__ __align__(16) uint32_t slab[];
   __shared__ unsigned long long s_q;
   __shared__ C4LargeSmem<kC4LargeThreads> sh;
@@ -128,8 +140,7 @@ __global__ void __launch_bounds__(kC4LargeThreads)
     __syncthreads();
     if (q >= nlist) break;
     const vid_t v = list[q];
-    const eid_t b = rp[v];
-    const int cut = c4_lower_bound(col + b, (int)(rp[v + 1] - b), v);
+    const int cut = cuts[q];
     // the slab is exact for any number of slices, only slower: it also takes the apexes
     // that would rather count densely when there are no dense arrays
     if (SLAB && (!dense || c4_slab_slices(v, cut, words) <= kC4MaxSlices))
@@ -175,8 +186,8 @@ DenseCache g_dense_cache[64];
 
 }  // namespace
 
-// Classifies the apexes of g's rank CSR once: g->d_c4_small (any order) and g->d_c4_large
-// (descending wedge bound), with their lengths.
+// Classifies the apexes of g's rank CSR once: g->d_c4_small (any order), g->d_c4_mid and
+// g->d_c4_large (descending wedge bound, followed by the cut of each), with their lengths.
 int ensure_c4_apexes(jgpm_graph* g) {
   if (g->c4_nsmall >= 0) return JGPM_OK;
   int rc;
@@ -201,7 +212,7 @@ int ensure_c4_apexes(jgpm_graph* g) {
   int32_t *ds = nullptr, *dm = nullptr, *dl = nullptr;
   if (cudaMalloc(&ds, std::max<int64_t>(1, nsmall) * 4) != cudaSuccess ||
       cudaMalloc(&dm, std::max<int64_t>(1, nmid) * 4) != cudaSuccess ||
-      cudaMalloc(&dl, std::max<int64_t>(1, nlarge) * 4) != cudaSuccess) {
+      cudaMalloc(&dl, std::max<int64_t>(1, 2 * nlarge) * 4) != cudaSuccess) {
     cudaGetLastError();
     cudaFree(ds);
     cudaFree(dm);
@@ -225,6 +236,9 @@ int ensure_c4_apexes(jgpm_graph* g) {
     JGPM_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(
         tmp.p, tb, (const uint64_t*)lkey.p, (uint64_t*)lkey2.p, (const vid_t*)large.p, dl,
         (int)nlarge, 0, 64, s));
+    k_c4_cuts<<<grid_for_c4(nlarge), 256, 0, s>>>(g->d_rank_rowptr, g->d_rank_col, dl, nlarge,
+                                                 dl + nlarge);
+    JGPM_CUDA_TRY(cudaGetLastError());
   }
   g->c4_large_keys.resize((size_t)nlarge);
   if (nlarge)

@@ -53,13 +53,14 @@ struct C4CtaHash {
   int pad[2];
 };
 
-// Block-wide wedge layout of a CTA of up to NT threads: thread r owns the wedges
-// [off[r], off[r+1]) of the flattened range, read from col[bx[r] ..].
+// Block-wide wedge layout of a CTA of NT threads: the non-empty lists of the block, compacted;
+// list r holds the wedges [off[r], off[r+1]) of the flattened range, read from col[bx[r] ..].
 template <int NT>
 struct C4LargeSmem {
-  int cut, nt;
-  int off[NT + 1];  // exclusive offsets, off[NT] = total
+  int nnz, nt;      // non-empty lists; touched-list length (dense path)
+  int off[NT + 1];  // exclusive offsets, off[nnz] = total
   int wsum[NT / 32];
+  int wnz[NT / 32];
   eid_t bx[NT];
 };
 
@@ -195,22 +196,10 @@ __device__ __forceinline__ acc_t c4_small_apex(const eid_t* rp, const vid_t* col
 }
 
 
-// Binary lifting over a sorted shared-memory array (fixed trip count, top = largest power of
-// two <= n): two independent searches in lockstep, p = #{a[j] < x}.
-__device__ __forceinline__ void c4_count_below2(const int* a, int n, int top, int x0, int x1,
-                                                int& p0, int& p1) {
-  p0 = 0;
-  p1 = 0;
-  for (int step = top; step > 0; step >>= 1) {
-    if (p0 + step <= n && a[p0 + step - 1] < x0) p0 += step;
-    if (p1 + step <= n && a[p1 + step - 1] < x1) p1 += step;
-  }
-}
-
 // Lays out the wedges of one block of lower-ranked neighbours, one per thread: `len` wedges read
-// from col[start ..].  Exclusive block scan into sh.off (sh.off[NT] = total), which it returns.
-// Every thread of the CTA (blockDim.x == NT) calls it; it ends with a barrier.  A caller that
-// reads sh after it puts a barrier before the next call.
+// from col[start ..].  The non-empty lists are compacted in thread order and their offsets
+// scanned into sh.off; returns the total.  Every thread of the CTA (blockDim.x == NT) calls it;
+// it ends with a barrier.  A caller that reads sh after it puts a barrier before the next call.
 template <int NT>
 __device__ __forceinline__ int c4_block_layout(int len, eid_t start, C4LargeSmem<NT>& sh) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -220,33 +209,74 @@ __device__ __forceinline__ int c4_block_layout(int len, eid_t start, C4LargeSmem
     const int t = __shfl_up_sync(kFull, incl, o);
     if (lane >= o) incl += t;
   }
-  if (lane == 31) sh.wsum[warp] = incl;
+  const unsigned nz = __ballot_sync(kFull, len > 0);
+  if (lane == 31) {
+    sh.wsum[warp] = incl;
+    sh.wnz[warp] = __popc(nz);
+  }
   __syncthreads();
-  int wbase = 0;
-  for (int w = 0; w < warp; ++w) wbase += sh.wsum[w];
-  sh.off[tid] = wbase + incl - len;
-  sh.bx[tid] = start;
-  if (tid == NT - 1) sh.off[NT] = wbase + incl;
+  int wbase = 0, zbase = 0;
+  for (int w = 0; w < warp; ++w) {
+    wbase += sh.wsum[w];
+    zbase += sh.wnz[w];
+  }
+  if (len > 0) {
+    const int k = zbase + __popc(nz & ((1u << lane) - 1u));
+    sh.off[k] = wbase + incl - len;
+    sh.bx[k] = start;
+  }
+  if (tid == NT - 1) {
+    const int k = zbase + __popc(nz);
+    sh.off[k] = wbase + incl;
+    sh.nnz = k;
+  }
   __syncthreads();
-  return sh.off[NT];
+  return sh.off[sh.nnz];
 }
 
-// Calls visit(v3) once for each of the T wedges of the layout, spread over all threads, two per
-// thread and iteration (so a hub x does not hold up one warp).  rows = number of threads that
-// own wedges (a prefix of the block).
+// Calls visit(v3) once for each of the T wedges of the layout.  Each warp takes a contiguous
+// run of 32-wedge chunks.  The list starts inside a chunk mark its bits in one OR-reduction, so
+// a lane finds the list of its wedge with a popcount instead of a search; the list of the next
+// chunk's first wedge follows from the same mask.  Coalesced: a warp reads 32 consecutive
+// wedges.
 template <int NT, typename Visit>
-__device__ __forceinline__ void c4_flat_wedges(const vid_t* col, const C4LargeSmem<NT>& sh,
-                                               int rows, int T, Visit visit) {
-  const int top = top_pow2_c4(rows - 1);
-  for (int t0 = threadIdx.x; t0 < T; t0 += 2 * NT) {
-    const bool two = t0 + NT < T;
-    const int t1 = two ? t0 + NT : t0;
-    int r0, r1;  // owner of wedge t = last r with off[r] <= t
-    c4_count_below2(sh.off + 1, rows - 1, top, t0 + 1, t1 + 1, r0, r1);
-    const vid_t a0 = __ldg(col + sh.bx[r0] + (t0 - sh.off[r0]));
-    const vid_t a1 = __ldg(col + sh.bx[r1] + (t1 - sh.off[r1]));
-    visit(a0);
-    if (two) visit(a1);
+__device__ __forceinline__ void c4_warp_wedges(const vid_t* col, const C4LargeSmem<NT>& sh,
+                                               int T, Visit visit) {
+  constexpr int kWarps = NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nnz = sh.nnz;
+  const int chunks = (T + 31) >> 5;
+  const int per = (chunks + kWarps - 1) / kWarps;
+  int c = warp * per;
+  const int cend = min(chunks, c + per);
+  if (c >= cend) return;
+  int t0 = c << 5;
+  int r0 = 0;  // last list with off[r0] <= t0 (off[0] = 0; offsets strictly increase)
+  for (int step = top_pow2_c4(nnz); step > 0; step >>= 1)
+    if (r0 + step < nnz && sh.off[r0 + step] <= t0) r0 += step;
+  for (; c < cend; ++c, t0 += 32) {
+    const int j = r0 + 1 + lane;  // lists after r0 start at positions >= 1 of the chunk
+    const int p = j <= nnz ? sh.off[j] - t0 : 64;
+    const unsigned m = __reduce_or_sync(kFull, (p > 0 && p < 32) ? (1u << p) : 0u);
+    const bool next_at_32 = __any_sync(kFull, p == 32);
+    const int r = r0 + __popc(m & (0xffffffffu >> (31 - lane)));
+    const int t = t0 + lane;
+    if (t < T) visit(__ldg(col + sh.bx[r] + (t - sh.off[r])));
+    r0 += __popc(m) + (next_at_32 ? 1 : 0);
+  }
+}
+
+// Lower bounds of K keys in one sorted list in lockstep (K independent loads per step):
+// p[i] = #{a[j] < key[i]}.
+template <int K>
+__device__ __forceinline__ void c4_lower_bounds(const vid_t* a, int n, const vid_t (&key)[K],
+                                                int (&p)[K]) {
+#pragma unroll
+  for (int i = 0; i < K; ++i) p[i] = 0;
+  for (int step = top_pow2_c4(n); step > 0; step >>= 1) {
+#pragma unroll
+    for (int i = 0; i < K; ++i)
+      if (p[i] + step <= n && __ldg(a + p[i] + step - 1) < key[i]) p[i] += step;
   }
 }
 
@@ -280,7 +310,7 @@ __device__ __forceinline__ acc_t c4_mid_apex(const eid_t* rp, const vid_t* col, 
       len = c4_lower_bound(col + bx, (int)(rp[x + 1] - bx), v);
     }
     const int T = c4_block_layout<NT>(len, bx, m.f);
-    c4_flat_wedges<NT>(col, m.f, min(NT, cut - base), T, [&](vid_t v3) {
+    c4_warp_wedges<NT>(col, m.f, T, [&](vid_t v3) {
       sum += (acc_t)c4_hash_add<kC4MidSlots, 20>(m.h.keys, m.h.cnt, m.h.used, &m.h.nused, v3);
     });
     __syncthreads();
@@ -319,7 +349,7 @@ __device__ __forceinline__ acc_t c4_large_apex(const eid_t* rp, const vid_t* col
       len = c4_lower_bound(col + bx, (int)(rp[x + 1] - bx), v);
     }
     const int T = c4_block_layout<NT>(len, bx, sh);
-    c4_flat_wedges<NT>(col, sh, min(NT, cut - base), T, [&](vid_t v3) {
+    c4_warp_wedges<NT>(col, sh, T, [&](vid_t v3) {
       const int old = atomicAdd(&dense[v3], 1);
       if (old == 0) touched[atomicAdd(&sh.nt, 1)] = v3;
       sum += (acc_t)old;
@@ -343,12 +373,15 @@ __device__ __forceinline__ void c4_slab_zero(uint32_t* slab, int words) {
 // a shared-memory slab of `words` words (zero on entry, zero again on return).  The counters are
 // packed 32 / 2^lgb to a word (c4_slab_lgbits: no count overflows its field), and the endpoint
 // range [0, v) is swept in slices of words * 32 / 2^lgb ids.  Each prefix(N(x), v) is sorted, so
-// one binary search per (x, slice) gives the wedges of the slice and no wedge is read twice.
-// Every thread calls it.  Returns this thread's share of sum C(c, 2).
+// binary searches for the slice boundaries give the wedges of each slice and no wedge is read
+// twice; with one block of x and at most kC4MaxSlices slices a thread finds all of its
+// boundaries in one lockstep search.  Every thread calls it.  Returns this thread's share of
+// sum C(c, 2).
 template <int NT>
 __device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col, vid_t v,
                                               int cut, uint32_t* slab, int words,
                                               C4LargeSmem<NT>& sh) {
+  static_assert(kC4MaxSlices == 4, "the lockstep boundary search holds four slices");
   const int tid = threadIdx.x;
   const eid_t b = rp[v];
   const int lgb = c4_slab_lgbits(cut);
@@ -357,16 +390,21 @@ __device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col,
   const uint32_t cmask = lgb == 5 ? 0xffffffffu : (1u << (1 << lgb)) - 1u;
   const int64_t span = (int64_t)words << lgper;
   const int nblk = (cut + NT - 1) / NT;
-  // one block of x: this thread's x list and its cursor, kept across the slices
+  const bool held = nblk == 1 && c4_slab_slices(v, cut, words) <= kC4MaxSlices;
+  // held: this thread's x list and the ends e[s] of its wedges in slices 0..3
   eid_t xb = 0;
-  int xd = 0, cur = 0;
-  if (nblk == 1 && tid < cut) {
+  int e[4] = {0, 0, 0, 0};
+  if (held && tid < cut) {
     const vid_t x = __ldg(col + b + tid);
     xb = rp[x];
-    xd = (int)(rp[x + 1] - xb);
+    vid_t key[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) key[i] = (vid_t)min((int64_t)v, (int64_t)(i + 1) * span);
+    c4_lower_bounds<4>(col + xb, (int)(rp[x + 1] - xb), key, e);
   }
   acc_t sum = 0;
-  for (int64_t lo = 0; lo < (int64_t)v; lo += span) {
+  int s = 0;
+  for (int64_t lo = 0; lo < (int64_t)v; lo += span, ++s) {
     const vid_t lo32 = (vid_t)lo;
     const vid_t hi = (vid_t)(lo + span < (int64_t)v ? lo + span : (int64_t)v);
     int added = 0;
@@ -375,23 +413,24 @@ __device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col,
       int len = 0;
       eid_t start = 0;
       if (i < cut) {
-        if (nblk == 1) {
-          const int e = cur + c4_lower_bound(col + xb + cur, xd - cur, hi);
-          start = xb + cur;
-          len = e - cur;
-          cur = e;
+        if (held) {
+          const int s0 = s == 0 ? 0 : s == 1 ? e[0] : s == 2 ? e[1] : e[2];
+          const int s1 = s == 0 ? e[0] : s == 1 ? e[1] : s == 2 ? e[2] : e[3];
+          start = xb + s0;
+          len = s1 - s0;
         } else {
           const vid_t x = __ldg(col + b + i);
           const eid_t bx = rp[x];
-          const int dx = (int)(rp[x + 1] - bx);
-          const int s0 = lo32 == 0 ? 0 : c4_lower_bound(col + bx, dx, lo32);
-          start = bx + s0;
-          len = c4_lower_bound(col + start, dx - s0, hi);
+          const vid_t key[2] = {lo32, hi};
+          int p[2];
+          c4_lower_bounds<2>(col + bx, (int)(rp[x + 1] - bx), key, p);
+          start = bx + p[0];
+          len = p[1] - p[0];
         }
       }
       const int T = c4_block_layout<NT>(len, start, sh);
       if (T > 0) {
-        c4_flat_wedges<NT>(col, sh, min(NT, cut - blk * NT), T, [&](vid_t v3) {
+        c4_warp_wedges<NT>(col, sh, T, [&](vid_t v3) {
           const uint32_t l = (uint32_t)(v3 - lo32);
           const int sft = (int)(l & lmask) << lgb;
           const uint32_t old = atomicAdd(slab + (l >> lgper), 1u << sft);
@@ -404,7 +443,7 @@ __device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col,
     if (added > 0) {
       if (nblk == 1 && added <= (words >> 4)) {
         // few wedges: zero the words they touched (the layout of the one block is still in sh)
-        c4_flat_wedges<NT>(col, sh, min(NT, cut), added, [&](vid_t v3) {
+        c4_warp_wedges<NT>(col, sh, added, [&](vid_t v3) {
           slab[(uint32_t)(v3 - lo32) >> lgper] = 0u;
         });
       } else {

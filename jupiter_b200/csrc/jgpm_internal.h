@@ -81,7 +81,7 @@ struct jgpm_graph {
   // hash and large (slab or dense counter) classes, the last sorted by descending bound
   int32_t* d_c4_small = nullptr;
   int32_t* d_c4_mid = nullptr;
-  int32_t* d_c4_large = nullptr;
+  int32_t* d_c4_large = nullptr;  // c4_nlarge apexes, then the cut of each
   int64_t c4_nsmall = -1;  // -1 = not built
   int64_t c4_nmid = 0;
   int64_t c4_nlarge = 0;
