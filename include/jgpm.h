@@ -197,8 +197,8 @@ typedef struct {
 
 /* Counts every job exactly in one persistent work-stealing launch: all jobs' work is cut into
  * tasks of one global queue that persistent CTAs drain; counts[i] receives job i's count.  The
- * large 4-cycle apexes of all jobs form a second queue, drained concurrently by a second
- * persistent kernel with wider CTAs.
+ * large 4-cycle apexes of all jobs form a second queue, drained first, on the same stream, by a
+ * second persistent kernel whose CTAs hold a shared-memory counter slab.
  * Replaces, for a whole batch, the reference's per-query round loop and static chunking
  * (src/jupiter_gpm.cu:356-375).  tuning = NULL uses the defaults.  All graphs must be on one
  * device. */

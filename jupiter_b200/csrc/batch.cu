@@ -17,7 +17,9 @@
 //   LARGE_ROOT  one root with d > kBatchWideMaxDeg, edge-rooted lists in warp scratch;
 //   C4_SMALL    4-cycle apexes with few wedges, one per warp (shared-memory hash);
 //   C4_MID      4-cycle apexes with up to 2048 wedges, each on the whole CTA (shared hash);
-//   C4_LARGE    one heavy 4-cycle apex on the whole CTA (dense counters in global memory).
+//   C4_LARGE    a heavy 4-cycle apex, or a run of lighter ones, on the whole CTA of the second
+//               kernel (shared-memory counter slab; dense counters in global memory past the
+//               slice cap).
 // Diamond jobs (reference P2, sum over edges of C(t_e, 2)) run the k = 3 root tasks in pair
 // mode: every triangle increments its three arcs' counters in the job's tri[] array and the
 // adds' old values give the pairs, so the count comes out of the same single pass.  Jobs for
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
 }
 
 // Large 4-cycle apexes of every 4-cycle job of the batch, heaviest first, on CTAs of 1024
-// threads, launched next to k_batch on a second stream.  Each CTA has a shared-memory slab of
+// threads, launched before k_batch on the same stream.  Each CTA has a shared-memory slab of
 // `words` words; an apex that needs more than kC4MaxSlices slices counts in the CTA's dense
 // array (and touched list) of `stride` ints instead when the batch has them.
 struct C4BatchArgs {
@@ -349,6 +351,8 @@ struct C4BatchArgs {
 };
 
 constexpr int kBatchC4Threads = 1024;
+constexpr uint64_t kC4TaskWedges = 1u << 16;  // wedge bound of a run of light large apexes
+constexpr int64_t kC4MidPerTask = 16;
 
 __global__ void __launch_bounds__(kBatchC4Threads) k_batch_c4_large(C4BatchArgs a) {
   extern __shared__ __align__(16) uint32_t slab[];
@@ -365,13 +369,15 @@ __global__ void __launch_bounds__(kBatchC4Threads) k_batch_c4_large(C4BatchArgs 
     if (q >= a.ntasks) break;
     const Task t = a.tasks[q];
     const JobDesc j = a.jobs[t.job];
-    const vid_t v = j.apexes[t.b];
-    const int cut = j.apexes[j.nlarge + t.b];
-    acc_t c;
-    if (!dense || c4_slab_slices(v, cut, a.words) <= kC4MaxSlices)
-      c = c4_slab_apex<kBatchC4Threads>(j.rrow, j.rcol, v, cut, slab, a.words, sh);
-    else
-      c = c4_large_apex<kBatchC4Threads>(j.rrow, j.rcol, v, cut, dense, touched, sh);
+    acc_t c = 0;
+    for (int64_t p = t.b; p < t.e; ++p) {
+      const vid_t v = j.apexes[p];
+      const int cut = j.apexes[j.nlarge + p];
+      if (!dense || c4_slab_slices(v, cut, a.words) <= kC4MaxSlices)
+        c += c4_slab_apex<kBatchC4Threads>(j.rrow, j.rcol, v, cut, slab, a.words, sh);
+      else
+        c += c4_large_apex<kBatchC4Threads>(j.rrow, j.rcol, v, cut, dense, touched, sh);
+    }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(&a.counts[t.job], c);
   }
@@ -433,12 +439,18 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
       jd.apexes = g->d_c4_large;
       jd.nlarge = (int32_t)g->c4_nlarge;
       jd.mid = g->d_c4_mid;
-      for (int64_t q = 0; q < g->c4_nlarge; ++q) {
-        c4l.push_back(Task{job, kTaskC4Large, q, q + 1});
-        c4w.push_back(g->c4_large_keys[(size_t)q]);
+      // large apexes (by descending wedge bound): a heavy one alone, lighter ones in runs of
+      // at most kC4TaskWedges of wedge bound
+      const std::vector<uint64_t>& key = g->c4_large_keys;
+      for (int64_t q = 0, e; q < g->c4_nlarge; q = e) {
+        uint64_t w = key[(size_t)q];
+        for (e = q + 1; e < g->c4_nlarge && w + key[(size_t)e] <= kC4TaskWedges; ++e)
+          w += key[(size_t)e];
+        c4l.push_back(Task{job, kTaskC4Large, q, e});
+        c4w.push_back(w);
       }
       if (g->c4_ndense > 0) o->c4max = std::max<int64_t>(o->c4max, g->n);
-      add_range_tasks(c4m, job, kTaskC4Mid, 0, g->c4_nmid, 2);
+      add_range_tasks(c4m, job, kTaskC4Mid, 0, g->c4_nmid, kC4MidPerTask);
       add_range_tasks(c4s, job, kTaskC4Small, 0, g->c4_nsmall, std::max<int64_t>(8, rpt / 8));
       c.h_jobs.push_back(jd);
       continue;
@@ -563,9 +575,10 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
                                   cudaMemcpyHostToDevice, s));
   JGPM_CUDA_TRY(cudaMemsetAsync(c.counts.p, 0, nj * sizeof(unsigned long long), s));
   JGPM_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, 2 * sizeof(unsigned long long), s));
-  // large 4-cycle apexes: k_batch_c4_large on the side stream, concurrently with k_batch
+  // large 4-cycle apexes: k_batch_c4_large on the same stream, before k_batch.  (Run side by
+  // side on two streams the two kernels took twice their sum: the persistent k_batch CTAs hold
+  // the SMs whose shared memory the slab CTAs need, and the two working sets share L2.)
   const size_t n4 = c.h_c4_tasks.size();
-  bool forked = false;
   if (n4 > 0) {
     const size_t slab_bytes = (size_t)kC4SlabWords * sizeof(uint32_t);
     if ((rc = raise_smem_limit((const void*)k_batch_c4_large, slab_bytes))) return rc;
@@ -588,9 +601,6 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     if ((rc = c.c4_tasks.reserve(n4 * sizeof(Task)))) return rc;
     JGPM_CUDA_TRY(cudaMemcpyAsync(c.c4_tasks.p, c.h_c4_tasks.data(), n4 * sizeof(Task),
                                   cudaMemcpyHostToDevice, s));
-    if ((rc = c.ensure_side_stream())) return rc;
-    JGPM_CUDA_TRY(cudaEventRecord(c.fork_ev, s));
-    JGPM_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork_ev, 0));
     C4BatchArgs b{};
     b.jobs = (const JobDesc*)c.jobs.p;
     b.tasks = (const Task*)c.c4_tasks.p;
@@ -601,10 +611,8 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     b.touched = need ? (vid_t*)c.c4t.p : nullptr;
     b.stride = o.c4max;
     b.words = kC4SlabWords;
-    k_batch_c4_large<<<(int)ctas, kBatchC4Threads, slab_bytes, c.side>>>(b);
+    k_batch_c4_large<<<(int)ctas, kBatchC4Threads, slab_bytes, s>>>(b);
     JGPM_CUDA_TRY(cudaGetLastError());
-    JGPM_CUDA_TRY(cudaEventRecord(c.join_ev, c.side));
-    forked = true;
   }
   a.jobs = (const JobDesc*)c.jobs.p;
   a.tasks = (const Task*)c.tasks.p;
@@ -616,7 +624,6 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   a.intersect = tu.intersect;
   if (nt) k_batch<<<grid, 256, smem, s>>>(a);
   JGPM_CUDA_TRY(cudaGetLastError());
-  if (forked) JGPM_CUDA_TRY(cudaStreamWaitEvent(s, c.join_ev, 0));
   if (h_counts)
     JGPM_CUDA_TRY(cudaMemcpyAsync(h_counts, c.counts.p, nj * sizeof(uint64_t),
                                   cudaMemcpyDeviceToHost, s));

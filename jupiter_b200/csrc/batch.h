@@ -25,7 +25,7 @@ enum TaskKind : int32_t {
   kTaskCtaRoot = 5,    // root b, split < d <= kBatchCtaMaxDeg, the whole CTA
   kTaskLargeRoot = 6,  // root b, d > kBatchWideMaxDeg, warps take its arcs (edge-rooted lists)
   kTaskC4Small = 7,    // small 4-cycle apexes [b, e) of the job's list, one per warp
-  kTaskC4Large = 8,    // large 4-cycle apex b of the job's list (k_batch_c4_large)
+  kTaskC4Large = 8,    // large 4-cycle apexes [b, e) of the job's list (k_batch_c4_large)
   kTaskC4Mid = 9,      // mid 4-cycle apexes [b, e) of the job's list, one after another per CTA
   kTaskWideRoot = 10,  // root b, kBatchCtaMaxDeg < d <= kBatchWideMaxDeg, the whole CTA with
                        // its bitmap rows in global scratch
@@ -87,30 +87,14 @@ struct BatchCtx {
   DevArena jobs, tasks, counts, cursor, c4, c4t, lists, tri, rows, c4_tasks;
   std::vector<JobDesc> h_jobs;
   std::vector<Task> h_tasks;
-  std::vector<Task> h_c4_tasks;  // large 4-cycle apexes, heaviest first
-  cudaStream_t side = nullptr;   // second stream of the large-apex kernel
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  std::vector<Task> h_c4_tasks;  // large 4-cycle apexes, by job, heaviest first
   std::vector<size_t> tri_off;  // diamond jobs: offset of the job's counters in `tri`
   size_t c4_zeroed = 0;
   size_t c4_cap_bytes = (size_t)4 << 30;  // memory cap of the 4-cycle counter arrays
-  int ensure_side_stream() {
-    if (side) return JGPM_OK;
-    if (cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming) != cudaSuccess) {
-      cudaGetLastError();
-      jgpm_set_error_("batch: stream/event creation failed");
-      return JGPM_ECUDA;
-    }
-    return JGPM_OK;
-  }
   ~BatchCtx() {
     for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &c4t, &lists, &tri, &rows,
                         &c4_tasks})
       if (d->p) cudaFree(d->p);
-    if (side) cudaStreamDestroy(side);
-    if (fork_ev) cudaEventDestroy(fork_ev);
-    if (join_ev) cudaEventDestroy(join_ev);
   }
 };
 
