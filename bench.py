@@ -542,6 +542,26 @@ def run_induced(args):
     print(json.dumps(out), flush=True)
 
 
+def run_count(args):
+    """One pattern on one seeded R-MAT graph, timed per count (device events): the command the
+    per-kernel profiles run.  --rmat n,ef,a,b,c,seed."""
+    import torch
+
+    import jupiter_b200 as J
+    torch.cuda.set_device(0)
+    f = args.rmat.split(",")
+    spec = (int(f[0]), int(f[1]), float(f[2]), float(f[3]), float(f[4]), int(f[5]))
+    with J.Graph.rmat(*spec) as g:
+        for _ in range(args.warmup):
+            c = g.count(args.pattern)
+        ms = []
+        for _ in range(args.steps):
+            c, st = g.count(args.pattern, details=True)
+            ms.append(st["kernel_ms"])
+        print(json.dumps({"workload": "count", "pattern": args.pattern, "rmat": list(spec),
+                          "count": c, "kernel_ms": ms, "graph": g.info()}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -551,7 +571,12 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="clique",
-                    choices=["clique", "batched", "served", "induced"])
+                    choices=["clique", "batched", "served", "induced", "count"])
+    ap.add_argument("--pattern", default="4-cycle")
+    ap.add_argument("--rmat",
+                    default="258730,32,0.471263918196369,0.13218402045090777,0.13218402045090777,2958",
+                    help="count workload: n,ef,a,b,c,seed (default: the heaviest 4-cycle job "
+                    "of the batched workload)")
     ap.add_argument("--jobs", type=int, default=4096)
     ap.add_argument("--plain-passes", type=int, default=1)
     ap.add_argument("--rates", type=float, nargs="+", default=[100, 300, 1000, 3000, 5000])
@@ -567,6 +592,8 @@ def main():
         run_served(args)
     elif args.workload == "induced":
         run_induced(args)
+    elif args.workload == "count":
+        run_count(args)
     else:
         run_jgpm(args)
 

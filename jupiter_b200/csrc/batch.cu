@@ -336,8 +336,9 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
 
 // Large 4-cycle apexes of every 4-cycle job of the batch, heaviest first, on CTAs of 1024
 // threads, launched before k_batch on the same stream.  Each CTA has a shared-memory slab of
-// `words` words; an apex that needs more than kC4MaxSlices slices counts in the CTA's dense
-// array (and touched list) of `stride` ints instead when the batch has them.
+// `words` words (kC4SlabWords, which the classifier's dense flags assume); an apex flagged dense
+// counts in the CTA's dense array (and touched list) of `stride` ints instead when the batch
+// has them.
 struct C4BatchArgs {
   const JobDesc* jobs;
   const Task* tasks;  // (job, apex index b)
@@ -350,33 +351,35 @@ struct C4BatchArgs {
   int words;
 };
 
-constexpr int kBatchC4Threads = 1024;
 constexpr uint64_t kC4TaskWedges = 1u << 16;  // wedge bound of a run of light large apexes
 constexpr int64_t kC4MidPerTask = 16;
 
-__global__ void __launch_bounds__(kBatchC4Threads) k_batch_c4_large(C4BatchArgs a) {
+__global__ void __launch_bounds__(kC4SlabThreads) k_batch_c4_large(C4BatchArgs a) {
   extern __shared__ __align__(16) uint32_t slab[];
-  __shared__ C4LargeSmem<kBatchC4Threads> sh;
-  __shared__ unsigned long long s_q;
+  __shared__ C4LargeSmem<kC4SlabThreads> sh;
+  __shared__ unsigned long long s_q[2];
   int32_t* dense = a.dense ? a.dense + (int64_t)blockIdx.x * a.stride : nullptr;
   vid_t* touched = a.dense ? a.touched + (int64_t)blockIdx.x * a.stride : nullptr;
-  c4_slab_zero<kBatchC4Threads>(slab, a.words);  // ordered by the barriers below
-  for (;;) {
-    if (threadIdx.x == 0) s_q = atomicAdd(a.cursor, 1ull);
-    __syncthreads();
-    const int64_t q = (int64_t)s_q;
-    __syncthreads();
+  c4_slab_zero<kC4SlabThreads>(slab, a.words);
+  if (threadIdx.x == 0) s_q[0] = atomicAdd(a.cursor, 1ull);
+  __syncthreads();
+  // double-buffered task fetch, as in the plain large-apex kernel: every task runs at least
+  // one apex, so barriers separate each slot's store from its reads
+  for (int it = 0;; ++it) {
+    const int64_t q = (int64_t)s_q[it & 1];
     if (q >= a.ntasks) break;
+    if (threadIdx.x == 0) s_q[(it + 1) & 1] = atomicAdd(a.cursor, 1ull);
     const Task t = a.tasks[q];
     const JobDesc j = a.jobs[t.job];
     acc_t c = 0;
     for (int64_t p = t.b; p < t.e; ++p) {
       const vid_t v = j.apexes[p];
-      const int cut = j.apexes[j.nlarge + p];
-      if (!dense || c4_slab_slices(v, cut, a.words) <= kC4MaxSlices)
-        c += c4_slab_apex<kBatchC4Threads>(j.rrow, j.rcol, v, cut, slab, a.words, sh);
+      const uint32_t cw = (uint32_t)j.apexes[j.nlarge + p];
+      const int cut = (int)(cw & ~kC4DenseFlag);
+      if (!dense || !(cw & kC4DenseFlag))
+        c += c4_slab_apex<kC4SlabThreads>(j.rrow, j.rcol, v, cut, slab, a.words, sh);
       else
-        c += c4_large_apex<kBatchC4Threads>(j.rrow, j.rcol, v, cut, dense, touched, sh);
+        c += c4_large_apex<kC4SlabThreads>(j.rrow, j.rcol, v, cut, dense, touched, sh);
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(&a.counts[t.job], c);
@@ -583,7 +586,7 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     const size_t slab_bytes = (size_t)kC4SlabWords * sizeof(uint32_t);
     if ((rc = raise_smem_limit((const void*)k_batch_c4_large, slab_bytes))) return rc;
     int c4_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c4_per_sm, k_batch_c4_large, kBatchC4Threads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c4_per_sm, k_batch_c4_large, kC4SlabThreads,
                                                   slab_bytes);
     int64_t ctas = std::min<int64_t>((int64_t)sms * std::max(1, c4_per_sm), (int64_t)n4);
     const size_t per_cta = (size_t)o.c4max * sizeof(int32_t);  // 0: no dense apex
@@ -611,7 +614,7 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     b.touched = need ? (vid_t*)c.c4t.p : nullptr;
     b.stride = o.c4max;
     b.words = kC4SlabWords;
-    k_batch_c4_large<<<(int)ctas, kBatchC4Threads, slab_bytes, s>>>(b);
+    k_batch_c4_large<<<(int)ctas, kC4SlabThreads, slab_bytes, s>>>(b);
     JGPM_CUDA_TRY(cudaGetLastError());
   }
   a.jobs = (const JobDesc*)c.jobs.p;

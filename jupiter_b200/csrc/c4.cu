@@ -10,9 +10,9 @@
 //   mid    (<= kC4MidBound)    one CTA per apex, counts in a CTA-wide shared-memory table;
 //   large                      one CTA of 1024 threads per apex, heaviest apexes first, the
 //                              counts in a shared-memory slab of packed counters swept over
-//                              the vertex range in at most kC4MaxSlices slices; an apex that
-//                              needs more slices (graphs of millions of vertices) counts in a
-//                              dense per-CTA array in global memory with a touched list.
+//                              the vertex range in slices; a light apex that would need many
+//                              slices (graphs of millions of vertices; c4_dense_apex) counts
+//                              in a dense per-CTA array in global memory with a touched list.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -50,9 +50,9 @@ __global__ void k_c4_classify(const eid_t* rp, const vid_t* col, vid_t n, vid_t*
       } else {
         const unsigned long long p = atomicAdd(&counters[1], 1ull);
         large_list[p] = (vid_t)v;
-        large_key[p] = ub;
-        if (c4_slab_slices((vid_t)v, cut, kC4SlabWords) > kC4MaxSlices)
-          atomicAdd(&counters[3], 1ull);
+        const bool dense = c4_dense_apex((vid_t)v, cut, ub, kC4SlabWords);
+        large_key[p] = ub | (dense ? 0ull : kC4SlabKey);
+        if (dense) atomicAdd(&counters[3], 1ull);
       }
     }
   }
@@ -77,14 +77,17 @@ __global__ void __launch_bounds__(256) k_c4_small(const eid_t* rp, const vid_t* 
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
 }
 
-// Lower-ranked neighbour count (the cut) of each large apex, stored after the apex list.
-__global__ void k_c4_cuts(const eid_t* rp, const vid_t* col, const vid_t* list, int64_t nlist,
-                          int32_t* cuts) {
+// Lower-ranked neighbour count (the cut) of each large apex, stored after the apex list with
+// kC4DenseFlag set for the apexes that count densely; strips kC4SlabKey from the sorted keys.
+__global__ void k_c4_cuts(const eid_t* rp, const vid_t* col, const vid_t* list, uint64_t* key,
+                          int64_t nlist, uint32_t* cuts) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nlist; q += stride) {
     const vid_t v = list[q];
     const eid_t b = rp[v];
-    cuts[q] = c4_lower_bound(col + b, (int)(rp[v + 1] - b), v);
+    const int cut = c4_lower_bound(col + b, (int)(rp[v + 1] - b), v);
+    cuts[q] = (uint32_t)cut | ((key[q] & kC4SlabKey) ? 0u : kC4DenseFlag);
+    key[q] &= ~kC4SlabKey;
   }
 }
 
@@ -112,41 +115,39 @@ __global__ void __launch_bounds__(kC4MidThreads) k_c4_mid(const eid_t* rp, const
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
 }
 
-// 1024 threads per CTA: one slab (or one dense array) is shared by as many warps as a CTA
-// holds, to keep enough atomics in flight.
-constexpr int kC4LargeThreads = 1024;
-
-// Large apexes.  words > 0: each CTA has a shared-memory slab of `words` words, used by every
-// apex that needs at most kC4MaxSlices slices; the other apexes count in the CTA's dense
-// array (counters: 2n ints per CTA, n counters then n touched ids; null when no apex needs
-// one).  SLAB == false: every apex counts densely (a lighter kernel, two CTAs per SM).
+// Large apexes on CTAs of kC4SlabThreads (1024) threads, so that one slab (or one dense array)
+// is shared by as many warps as a CTA holds.  SLAB: every apex of the list counts in the CTA's
+// shared-memory slab of `words` words (one CTA per SM).  Otherwise every apex counts in the
+// CTA's dense array (counters: 2n ints per CTA, n counters then n touched ids), a lighter
+// kernel with two CTAs per SM.  cuts: the stored cut of each apex of the list.
 template <bool SLAB>
-__global__ void __launch_bounds__(kC4LargeThreads)
-    k_c4_large(const eid_t* rp, const vid_t* col, vid_t n, const vid_t* list, int64_t nlist,
-               unsigned long long* cursor, int32_t* counters, int words, DevControl* ctl) {
-  const int32_t* cuts = list + nlist;
+__global__ void __launch_bounds__(kC4SlabThreads)
+    k_c4_large(const eid_t* rp, const vid_t* col, vid_t n, const vid_t* list,
+               const uint32_t* cuts, int64_t nlist, unsigned long long* cursor,
+               int32_t* counters, int words, DevControl* ctl) {
   extern __shared__ __align__(16) uint32_t slab[];
-  __shared__ unsigned long long s_q;
-  __shared__ C4LargeSmem<kC4LargeThreads> sh;
-  int32_t* dense = counters ? counters + (int64_t)blockIdx.x * 2 * n : nullptr;
-  vid_t* touched = counters ? dense + n : nullptr;
+  __shared__ unsigned long long s_q[2];
+  __shared__ C4LargeSmem<kC4SlabThreads> sh;
+  int32_t* dense = SLAB ? nullptr : counters + (int64_t)blockIdx.x * 2 * n;
+  vid_t* touched = SLAB ? nullptr : dense + n;
   const int tid = threadIdx.x, lane = tid & 31;
-  if (SLAB) c4_slab_zero<kC4LargeThreads>(slab, words);  // ordered by the barriers below
+  if (SLAB) c4_slab_zero<kC4SlabThreads>(slab, words);
+  if (tid == 0) s_q[0] = atomicAdd(cursor, 1ull);
+  __syncthreads();
   acc_t sum = 0;
-  for (;;) {
-    if (tid == 0) s_q = atomicAdd(cursor, 1ull);
-    __syncthreads();
-    const int64_t q = (int64_t)s_q;
-    __syncthreads();
+  // Double-buffered task fetch: thread 0 takes the next apex while this one runs; every apex
+  // passes barriers (its layouts) between the store and the reads of the next slot, and
+  // between the reads of this slot and its next store.
+  for (int it = 0;; ++it) {
+    const int64_t q = (int64_t)s_q[it & 1];
     if (q >= nlist) break;
+    if (tid == 0) s_q[(it + 1) & 1] = atomicAdd(cursor, 1ull);
     const vid_t v = list[q];
-    const int cut = cuts[q];
-    // the slab is exact for any number of slices, only slower: it also takes the apexes
-    // that would rather count densely when there are no dense arrays
-    if (SLAB && (!dense || c4_slab_slices(v, cut, words) <= kC4MaxSlices))
-      sum += c4_slab_apex<kC4LargeThreads>(rp, col, v, cut, slab, words, sh);
+    const int cut = (int)(cuts[q] & ~kC4DenseFlag);
+    if (SLAB)
+      sum += c4_slab_apex<kC4SlabThreads>(rp, col, v, cut, slab, words, sh);
     else
-      sum += c4_large_apex<kC4LargeThreads>(rp, col, v, cut, dense, touched, sh);
+      sum += c4_large_apex<kC4SlabThreads>(rp, col, v, cut, dense, touched, sh);
   }
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
@@ -236,8 +237,9 @@ int ensure_c4_apexes(jgpm_graph* g) {
     JGPM_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(
         tmp.p, tb, (const uint64_t*)lkey.p, (uint64_t*)lkey2.p, (const vid_t*)large.p, dl,
         (int)nlarge, 0, 64, s));
-    k_c4_cuts<<<grid_for_c4(nlarge), 256, 0, s>>>(g->d_rank_rowptr, g->d_rank_col, dl, nlarge,
-                                                 dl + nlarge);
+    k_c4_cuts<<<grid_for_c4(nlarge), 256, 0, s>>>(g->d_rank_rowptr, g->d_rank_col, dl,
+                                                 (uint64_t*)lkey2.p, nlarge,
+                                                 (uint32_t*)(dl + nlarge));
     JGPM_CUDA_TRY(cudaGetLastError());
   }
   g->c4_large_keys.resize((size_t)nlarge);
@@ -262,29 +264,26 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
   const int32_t n = g->n;
   const int sms = device_sm_count(g->device);
   const int64_t nsmall = g->c4_nsmall, nmid = g->c4_nmid, nlarge = g->c4_nlarge;
-  // Large apexes: a shared-memory slab per CTA when any apex fits one (one CTA per SM), and
-  // dense counters and touched lists (2n ints per CTA, within a 12 GiB cap) only when some
-  // apex needs more slices than allowed.  The dense arrays are allocated for this count only
-  // (a graph pool would otherwise keep one such array set per graph), or taken from a small
-  // per-device cache.
-  const int64_t ndense = g->c4_ndense;
-  const int words = nlarge > ndense ? kC4SlabWords : 0;
-  const size_t slab_bytes = (size_t)words * sizeof(uint32_t);
-  int64_t ctas = 0;
-  if (nlarge > 0) {
-    int per_sm = 2;
-    if (words > 0) {
-      if ((rc = raise_smem_limit((const void*)k_c4_large<true>, slab_bytes))) return rc;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_large<true>, kC4LargeThreads,
-                                                    slab_bytes);
-      per_sm = std::max(1, per_sm);
-    }
-    ctas = (int64_t)sms * per_sm;
+  // Large apexes: the slab ones (first in the list) on one CTA per SM with a shared-memory slab,
+  // then the dense ones on two CTAs per SM with dense counters and touched lists (2n ints per
+  // CTA, within a 12 GiB cap).  The dense arrays are allocated for this count only (a graph
+  // pool would otherwise keep one such array set per graph), or taken from a small per-device
+  // cache.
+  const int64_t ndense = g->c4_ndense, nslab = nlarge - ndense;
+  const uint32_t* cuts = (const uint32_t*)(g->d_c4_large + nlarge);
+  const size_t slab_bytes = (size_t)kC4SlabWords * sizeof(uint32_t);
+  int64_t slab_ctas = 0;
+  if (nslab > 0) {
+    if ((rc = raise_smem_limit((const void*)k_c4_large<true>, slab_bytes))) return rc;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_large<true>, kC4SlabThreads,
+                                                  slab_bytes);
+    slab_ctas = std::min<int64_t>((int64_t)sms * std::max(1, per_sm), nslab);
   }
   const int64_t per_cta = (int64_t)n * 8;
-  if (ndense > 0)
-    ctas = std::min<int64_t>(ctas, ((int64_t)12 << 30) / std::max<int64_t>(1, per_cta));
-  ctas = std::max<int64_t>(1, std::min<int64_t>(ctas, nlarge));
+  int64_t ctas = std::min<int64_t>((int64_t)sms * 2,
+                                   ((int64_t)12 << 30) / std::max<int64_t>(1, per_cta));
+  ctas = std::max<int64_t>(1, std::min<int64_t>(ctas, ndense));
   const size_t dense_bytes = ndense > 0 ? (size_t)(ctas * per_cta) : 0;
   TmpBuf dense_tmp;
   std::unique_lock<std::mutex> cache_lk;
@@ -335,12 +334,17 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
                                           &g->d_ctl->counter[2], g->d_ctl);
     g->launches += 1;
   }
-  if (nlarge > 0) {
-    if (dense_bytes) JGPM_CUDA_TRY(cudaMemsetAsync(dense, 0, dense_bytes, s));
-    auto kern = words > 0 ? k_c4_large<true> : k_c4_large<false>;
-    kern<<<(int)ctas, kC4LargeThreads, slab_bytes, s>>>(
-        g->d_rank_rowptr, g->d_rank_col, n, g->d_c4_large, nlarge, &g->d_ctl->counter[1],
-        (int32_t*)dense, words, g->d_ctl);
+  if (nslab > 0) {
+    k_c4_large<true><<<(int)slab_ctas, kC4SlabThreads, slab_bytes, s>>>(
+        g->d_rank_rowptr, g->d_rank_col, n, g->d_c4_large, cuts, nslab, &g->d_ctl->counter[1],
+        nullptr, kC4SlabWords, g->d_ctl);
+    g->launches += 1;
+  }
+  if (ndense > 0) {
+    JGPM_CUDA_TRY(cudaMemsetAsync(dense, 0, dense_bytes, s));
+    k_c4_large<false><<<(int)ctas, kC4SlabThreads, 0, s>>>(
+        g->d_rank_rowptr, g->d_rank_col, n, g->d_c4_large + nslab, cuts + nslab, ndense,
+        &g->d_ctl->counter[3], (int32_t*)dense, 0, g->d_ctl);
     g->launches += 1;
   }
   cudaEventRecord(e1, s);

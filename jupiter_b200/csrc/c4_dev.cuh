@@ -24,9 +24,8 @@ namespace jgpm {
 //   small  ub <= kC4SmallBound  one warp, shared-memory hash of kC4HashSlots (load <= 1/2);
 //   mid    ub <= kC4MidBound    one CTA, shared-memory hash of kC4MidSlots (load <= 1/2);
 //   large                       one CTA of 1024 threads, either a shared-memory slab of packed
-//                               counters swept over the vertex range in at most kC4MaxSlices
-//                               slices, or (more slices) a dense counter array in global
-//                               memory.
+//                               counters swept over the vertex range in slices, or a dense
+//                               counter array in global memory (c4_dense_apex).
 constexpr int kC4SmallBound = 256;
 constexpr int kC4HashSlots = 512;
 constexpr int kC4MidBound = 2048;
@@ -82,6 +81,30 @@ __host__ __device__ __forceinline__ int64_t c4_slab_slices(vid_t v, int cut, int
   const int64_t span = (int64_t)words << (5 - c4_slab_lgbits(cut));
   return ((int64_t)v + span - 1) / span;
 }
+
+// Threads of a large-apex CTA (slab and dense kernels, plain and batched).
+constexpr int kC4SlabThreads = 1024;
+
+// Whether a large apex counts in a dense global array rather than in the slab.  The slab costs
+// a layout and a boundary search per x for every (slice, block of kC4SlabThreads x), so an
+// apex takes it when it needs at most kC4MaxSlices slices or brings at least kC4SliceWedges of
+// wedge bound per (slice, block).  (Dense counters of a graph of millions of vertices do not
+// stay in L2: every wedge then costs an atomic in DRAM, about ten times a slab add.)  The
+// classifier decides with this one function and records it with the apex.
+constexpr uint64_t kC4SliceWedges = 1024;
+__host__ __device__ __forceinline__ bool c4_dense_apex(vid_t v, int cut, uint64_t ub,
+                                                       int words) {
+  const int64_t sl = c4_slab_slices(v, cut, words);
+  const int64_t nblk = ((int64_t)cut + kC4SlabThreads - 1) / kC4SlabThreads;
+  return sl > kC4MaxSlices && ub < (uint64_t)(sl * nblk) * kC4SliceWedges;
+}
+
+// Sort key of a large apex: its wedge bound, with kC4SlabKey set for slab apexes, so that a
+// descending sort puts the slab apexes first and the dense ones after, each by bound.
+constexpr uint64_t kC4SlabKey = 1ull << 63;
+
+// The cut of a large apex as stored after the apex list: bit 31 set for a dense apex.
+constexpr uint32_t kC4DenseFlag = 0x80000000u;
 
 __device__ __forceinline__ int top_pow2_c4(int n) { return n > 0 ? 1 << (31 - __clz(n)) : 0; }
 
@@ -375,8 +398,9 @@ __device__ __forceinline__ void c4_slab_zero(uint32_t* slab, int words) {
 // range [0, v) is swept in slices of words * 32 / 2^lgb ids.  Each prefix(N(x), v) is sorted, so
 // binary searches for the slice boundaries give the wedges of each slice and no wedge is read
 // twice; with one block of x and at most kC4MaxSlices slices a thread finds all of its
-// boundaries in one lockstep search.  Every thread calls it.  Returns this thread's share of
-// sum C(c, 2).
+// boundaries in one lockstep search.  Every thread calls it.  It may return before the last
+// clearing stores of other threads are done: the caller's next access to the slab or to sh
+// must follow a c4_block_layout (or a barrier).  Returns this thread's share of sum C(c, 2).
 template <int NT>
 __device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col, vid_t v,
                                               int cut, uint32_t* slab, int words,
@@ -390,17 +414,23 @@ __device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col,
   const uint32_t cmask = lgb == 5 ? 0xffffffffu : (1u << (1 << lgb)) - 1u;
   const int64_t span = (int64_t)words << lgper;
   const int nblk = (cut + NT - 1) / NT;
-  const bool held = nblk == 1 && c4_slab_slices(v, cut, words) <= kC4MaxSlices;
-  // held: this thread's x list and the ends e[s] of its wedges in slices 0..3
+  const bool one = nblk == 1;
+  const bool held = one && c4_slab_slices(v, cut, words) <= kC4MaxSlices;
+  // one block: this thread's x list stays in registers; held: with the ends e[s] of its
+  // wedges in slices 0..3, else with a cursor that each slice's search starts from
   eid_t xb = 0;
+  int xd = 0, cur = 0;
   int e[4] = {0, 0, 0, 0};
-  if (held && tid < cut) {
+  if (one && tid < cut) {
     const vid_t x = __ldg(col + b + tid);
     xb = rp[x];
-    vid_t key[4];
+    xd = (int)(rp[x + 1] - xb);
+    if (held) {
+      vid_t key[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) key[i] = (vid_t)min((int64_t)v, (int64_t)(i + 1) * span);
-    c4_lower_bounds<4>(col + xb, (int)(rp[x + 1] - xb), key, e);
+      for (int i = 0; i < 4; ++i) key[i] = (vid_t)min((int64_t)v, (int64_t)(i + 1) * span);
+      c4_lower_bounds<4>(col + xb, xd, key, e);
+    }
   }
   acc_t sum = 0;
   int s = 0;
@@ -418,6 +448,11 @@ __device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col,
           const int s1 = s == 0 ? e[0] : s == 1 ? e[1] : s == 2 ? e[2] : e[3];
           start = xb + s0;
           len = s1 - s0;
+        } else if (one) {
+          const int s1 = cur + c4_lower_bound(col + xb + cur, xd - cur, hi);
+          start = xb + cur;
+          len = s1 - cur;
+          cur = s1;
         } else {
           const vid_t x = __ldg(col + b + i);
           const eid_t bx = rp[x];
@@ -449,7 +484,8 @@ __device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col,
       } else {
         c4_slab_zero<NT>(slab, ((int)(((uint32_t)(hi - lo32) + lmask) >> lgper) + 3) & ~3);
       }
-      __syncthreads();
+      // no barrier here: whatever touches the slab or sh next (the next slice, or the next
+      // apex) starts with a layout, whose barriers order it after these stores
     }
   }
   return sum;

@@ -85,7 +85,7 @@ struct jgpm_graph {
   int64_t c4_nsmall = -1;  // -1 = not built
   int64_t c4_nmid = 0;
   int64_t c4_nlarge = 0;
-  int64_t c4_ndense = 0;   // large apexes that need more slab slices than allowed
+  int64_t c4_ndense = 0;   // large apexes that count in dense arrays (c4_dense_apex)
   std::vector<uint64_t> c4_large_keys;  // host copy: wedge bound of each large apex, descending
   int32_t max_out_degree = 0;
   jgpm::RootTiers tiers;

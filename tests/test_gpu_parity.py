@@ -193,8 +193,8 @@ def test_large_roots_against_oracle(gpu):
 
 def c4_slab_graphs():
     """R-MAT graphs whose large 4-cycle apexes cover the slab forms: 2^18 vertices (two and
-    three slices, 8- and 16-bit counters) and 2^20 (the top-ranked apexes past the slice cap,
-    in dense arrays)."""
+    three slices, 8- and 16-bit counters) and 2^20 (up to eleven slices: the heavy top-ranked
+    apexes sweep them, the light ones count in dense arrays)."""
     return [(1 << 18, 8, 0.6, 0.1, 0.1, 11), (1 << 20, 4, 0.6, 0.1, 0.1, 11)]
 
 
