@@ -396,7 +396,7 @@ namespace {
 
 void add_range_tasks(std::vector<Task>& out, int job, int kind, int64_t b, int64_t e,
                      int64_t chunk) {
-  for (int64_t x = b; x < e; x += chunk) out.push_back(Task{job, kind, x, std::min(e, x + chunk)});
+  for (int64_t x = b; x < e; x += chunk) out.push_back(make_task(job, kind, x, std::min(e, x + chunk)));
 }
 
 // First index of the root tiers whose out-degree is <= x, x in {32, 64, 128, 256, 512}
@@ -420,8 +420,10 @@ struct BuildOut {
 int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchCtx& c,
                 BuildOut* o) {
   c.h_jobs.clear();
-  c.h_tasks.clear();
-  std::vector<Task> heavy, cta, warp, c4m, c4s, light, c4l;
+  for (std::vector<Task>& v : c.cls) v.clear();
+  c.h_c4_tasks.clear();
+  std::vector<Task>&heavy = c.cls[0], &cta = c.cls[1], &c4m = c.cls[2], &warp = c.cls[3],
+                     &c4s = c.cls[4], &light = c.cls[5], &c4l = c.h_c4_tasks;
   std::vector<uint64_t> c4w;  // wedge bound of each large-apex task
   std::vector<size_t> tri_off(in.size(), 0);
   const int split = tu.split_degree >= 128 ? 128 : tu.split_degree >= 64 ? 64 : 32;
@@ -449,7 +451,7 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
         uint64_t w = key[(size_t)q];
         for (e = q + 1; e < g->c4_nlarge && w + key[(size_t)e] <= kC4TaskWedges; ++e)
           w += key[(size_t)e];
-        c4l.push_back(Task{job, kTaskC4Large, q, e});
+        c4l.push_back(make_task(job, kTaskC4Large, q, e));
         c4w.push_back(w);
       }
       if (g->c4_ndense > 0) o->c4max = std::max<int64_t>(o->c4max, g->n);
@@ -478,16 +480,16 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
     const int64_t large_end = std::min(stop, tier_begin(t, kBatchCtaMaxDeg));
     const int64_t cta_end = std::min(stop, std::max(large_end, tier_begin(t, split)));
     const int64_t warp_end = std::min(stop, std::max(cta_end, t.deg_begin[32]));
-    for (int64_t r = 0; r < wide_begin; ++r) heavy.push_back(Task{job, kTaskLargeRoot, r, r + 1});
+    for (int64_t r = 0; r < wide_begin; ++r) heavy.push_back(make_task(job, kTaskLargeRoot, r, r + 1));
     if (wide_begin > 0) {
       o->any_large = true;
       o->max_out = std::max(o->max_out, g->max_out_degree);
     }
     for (int64_t r = wide_begin; r < large_end; ++r)
-      heavy.push_back(Task{job, kTaskWideRoot, r, r + 1});
+      heavy.push_back(make_task(job, kTaskWideRoot, r, r + 1));
     if (large_end > wide_begin)
       o->wdmax = std::max(o->wdmax, std::min(g->max_out_degree, kBatchWideMaxDeg));
-    for (int64_t r = large_end; r < cta_end; ++r) cta.push_back(Task{job, kTaskCtaRoot, r, r + 1});
+    for (int64_t r = large_end; r < cta_end; ++r) cta.push_back(make_task(job, kTaskCtaRoot, r, r + 1));
     if (cta_end > large_end)
       o->dmax = std::max(o->dmax, std::min(g->max_out_degree, kBatchCtaMaxDeg));
     add_range_tasks(warp, job, kTaskWarpRoots, cta_end, warp_end, std::max<int64_t>(8, rpt / 16));
@@ -519,11 +521,17 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
       return wx != wy ? wx > wy : x.job < y.job;
     });
   }
-  c.h_c4_tasks.swap(c4l);
-  c.h_tasks.reserve(heavy.size() + cta.size() + c4m.size() + warp.size() + c4s.size() +
-                    light.size());
-  for (auto* v : {&heavy, &cta, &c4m, &warp, &c4s, &light})
-    c.h_tasks.insert(c.h_tasks.end(), v->begin(), v->end());
+  size_t total = 0;
+  for (const std::vector<Task>& v : c.cls) total += v.size();
+  c.h_tasks.wait();  // the previous batch's copy out of the pinned table has finished
+  int rc2;
+  if ((rc2 = c.h_tasks.reserve(total))) return rc2;
+  size_t at = 0;
+  for (const std::vector<Task>& v : c.cls) {  // heavy, cta, c4m, warp, c4s, light
+    if (!v.empty()) memcpy(c.h_tasks.p + at, v.data(), v.size() * sizeof(Task));
+    at += v.size();
+  }
+  c.h_tasks.n = total;
   c.tri_off.swap(tri_off);
   return JGPM_OK;
 }
@@ -546,7 +554,7 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, 256, smem);
   per_sm = std::max(1, std::min(per_sm, 8));
   const int grid = sms * per_sm;
-  const size_t nj = c.h_jobs.size(), nt = c.h_tasks.size();
+  const size_t nj = c.h_jobs.size(), nt = c.h_tasks.n;
   if ((rc = c.jobs.reserve(nj * sizeof(JobDesc)))) return rc;
   if ((rc = c.tasks.reserve(std::max<size_t>(1, nt) * sizeof(Task)))) return rc;
   if ((rc = c.counts.reserve(nj * sizeof(unsigned long long)))) return rc;
@@ -574,8 +582,9 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   JGPM_CUDA_TRY(cudaMemcpyAsync(c.jobs.p, c.h_jobs.data(), nj * sizeof(JobDesc),
                                 cudaMemcpyHostToDevice, s));
   if (nt)
-    JGPM_CUDA_TRY(cudaMemcpyAsync(c.tasks.p, c.h_tasks.data(), nt * sizeof(Task),
+    JGPM_CUDA_TRY(cudaMemcpyAsync(c.tasks.p, c.h_tasks.p, nt * sizeof(Task),
                                   cudaMemcpyHostToDevice, s));
+  if ((rc = c.h_tasks.record(s))) return rc;
   JGPM_CUDA_TRY(cudaMemsetAsync(c.counts.p, 0, nj * sizeof(unsigned long long), s));
   JGPM_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, 2 * sizeof(unsigned long long), s));
   // large 4-cycle apexes: k_batch_c4_large on the same stream, before k_batch.  (Run side by

@@ -57,8 +57,12 @@ struct JobDesc {
 struct Task {
   int32_t job;
   int32_t kind;
-  int64_t b, e;
+  int32_t b, e;  // index range in the job's root or apex list
 };
+
+inline Task make_task(int job, int kind, int64_t b, int64_t e) {
+  return Task{(int32_t)job, (int32_t)kind, (int32_t)b, (int32_t)e};
+}
 
 // Growable device buffer.
 struct DevArena {
@@ -80,14 +84,62 @@ struct DevArena {
   }
 };
 
+// Pinned host copy of a batch's task table, from which the device copy is made.  `done`
+// marks the end of the last copy out of it: a new batch waits for it before writing.
+struct PinnedTasks {
+  Task* p = nullptr;
+  size_t cap = 0, n = 0;
+  cudaEvent_t done = nullptr;
+  bool pending = false;
+  void wait() {
+    if (pending) cudaEventSynchronize(done);
+    pending = false;
+  }
+  int reserve(size_t want) {
+    if (want <= cap) return JGPM_OK;
+    wait();
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    const size_t sz = std::max<size_t>(want + want / 4, (size_t)1 << 16);
+    if (cudaHostAlloc((void**)&p, sz * sizeof(Task), cudaHostAllocDefault) != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      jgpm_set_error_("batch: pinned host allocation failed");
+      return JGPM_ENOMEM;
+    }
+    cap = sz;
+    return JGPM_OK;
+  }
+  int record(cudaStream_t s) {
+    if (!done && cudaEventCreateWithFlags(&done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      jgpm_set_error_("batch: event creation failed");
+      return JGPM_ECUDA;
+    }
+    if (cudaEventRecord(done, s) != cudaSuccess) {
+      jgpm_set_error_("batch: event record failed");
+      return JGPM_ECUDA;
+    }
+    pending = true;
+    return JGPM_OK;
+  }
+  ~PinnedTasks() {
+    wait();
+    if (p) cudaFreeHost(p);
+    if (done) cudaEventDestroy(done);
+  }
+};
+
 // Reusable per-device launch state of the batched kernel (task/job tables, counters,
 // scratch).  One per server slot or per synchronous caller.
 struct BatchCtx {
   int device = 0;
   DevArena jobs, tasks, counts, cursor, c4, c4t, lists, tri, rows, c4_tasks;
   std::vector<JobDesc> h_jobs;
-  std::vector<Task> h_tasks;
+  PinnedTasks h_tasks;           // the main queue
   std::vector<Task> h_c4_tasks;  // large 4-cycle apexes, by job, heaviest first
+  std::vector<Task> cls[6];      // per-class task lists while building (capacity kept)
   std::vector<size_t> tri_off;  // diamond jobs: offset of the job's counters in `tri`
   size_t c4_zeroed = 0;
   size_t c4_cap_bytes = (size_t)4 << 30;  // memory cap of the 4-cycle counter arrays
