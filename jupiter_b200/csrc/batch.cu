@@ -171,20 +171,33 @@ __device__ __forceinline__ acc_t task_warp_roots(const JobDesc& j, int64_t b, in
   }
 }
 
+// Row-mask width counted from registers for a CTA root band of up to W words (the plain
+// bands' widths; the register-mask recursion is left out of k >= 7 as in the plain kernels).
+template <int K, int W>
+constexpr int batch_row_words() { return K >= 7 || (K >= 6 && W > 8) ? 0 : W; }
+
+// One CTA root with rows of up to W words (out-degree <= 32 W), masks in registers.
+template <int W>
 __device__ __forceinline__ acc_t task_cta_root(const JobDesc& j, vid_t u, const MidSmem& sm) {
   acc_t el = 0;
-  if (j.kind == kJobDiamond)
+  if (j.kind == kJobDiamond)  // pair mode returns before the mask counting
     return cta_root<3, false, true, true, 0>(j.drow, j.dcol, u, sm, j.tri, el);
   if (j.kind == kJobIndTT)
-    return cta_root<4, false, true, true, 0, 1, false, true>(j.drow, j.dcol, u, sm, j.tri, el,
+    return cta_root<4, false, true, true, W, 1, false, true>(j.drow, j.dcol, u, sm, j.tri, el,
                                                              j.srow);
   switch (j.k) {
-    case 3: return cta_root<3, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
-    case 4: return cta_root<4, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
-    case 5: return cta_root<5, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
-    case 6: return cta_root<6, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
-    case 7: return cta_root<7, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
-    default: return cta_root<8, false, false, false, 0>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 3: return cta_root<3, false, false, false, W>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 4: return cta_root<4, false, false, false, W>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 5: return cta_root<5, false, false, false, W>(j.drow, j.dcol, u, sm, nullptr, el);
+    case 6:
+      return cta_root<6, false, false, false, batch_row_words<6, W>()>(j.drow, j.dcol, u, sm,
+                                                                       nullptr, el);
+    case 7:
+      return cta_root<7, false, false, false, batch_row_words<7, W>()>(j.drow, j.dcol, u, sm,
+                                                                       nullptr, el);
+    default:
+      return cta_root<8, false, false, false, batch_row_words<8, W>()>(j.drow, j.dcol, u, sm,
+                                                                       nullptr, el);
   }
 }
 
@@ -304,7 +317,11 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
         break;
       case kTaskCtaRoot:
         smem_kind = kTaskCtaRoot;
-        c = task_cta_root(j, j.roots[t.b], sm);
+        c = task_cta_root<16>(j, j.roots[t.b], sm);
+        break;
+      case kTaskCtaRoot8:
+        smem_kind = kTaskCtaRoot;
+        c = task_cta_root<8>(j, j.roots[t.b], sm);
         break;
       case kTaskWideRoot: {
         smem_kind = kTaskWideRoot;
@@ -489,7 +506,10 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
       heavy.push_back(make_task(job, kTaskWideRoot, r, r + 1));
     if (large_end > wide_begin)
       o->wdmax = std::max(o->wdmax, std::min(g->max_out_degree, kBatchWideMaxDeg));
-    for (int64_t r = large_end; r < cta_end; ++r) cta.push_back(make_task(job, kTaskCtaRoot, r, r + 1));
+    // CTA roots above out-degree 256 count 16-word masks, the others 8-word ones
+    const int64_t cta16_end = std::min(cta_end, std::max(large_end, tier_begin(t, 256)));
+    for (int64_t r = large_end; r < cta_end; ++r)
+      cta.push_back(make_task(job, r < cta16_end ? kTaskCtaRoot : kTaskCtaRoot8, r, r + 1));
     if (cta_end > large_end)
       o->dmax = std::max(o->dmax, std::min(g->max_out_degree, kBatchCtaMaxDeg));
     add_range_tasks(warp, job, kTaskWarpRoots, cta_end, warp_end, std::max<int64_t>(8, rpt / 16));

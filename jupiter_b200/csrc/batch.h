@@ -22,13 +22,16 @@ enum TaskKind : int32_t {
   kTaskGroup16 = 2,
   kTaskGroup32 = 3,
   kTaskWarpRoots = 4,  // roots [b, e) of out-degree 32 < d <= split, one per warp
-  kTaskCtaRoot = 5,    // root b, split < d <= kBatchCtaMaxDeg, the whole CTA
+  kTaskCtaRoot = 5,    // root b, max(split, 256) < d <= kBatchCtaMaxDeg, the whole CTA, masks
+                       // of up to 16 words in registers
   kTaskLargeRoot = 6,  // root b, d > kBatchWideMaxDeg, warps take its arcs (edge-rooted lists)
   kTaskC4Small = 7,    // small 4-cycle apexes [b, e) of the job's list, one per warp
   kTaskC4Large = 8,    // large 4-cycle apexes [b, e) of the job's list (k_batch_c4_large)
   kTaskC4Mid = 9,      // mid 4-cycle apexes [b, e) of the job's list, one after another per CTA
   kTaskWideRoot = 10,  // root b, kBatchCtaMaxDeg < d <= kBatchWideMaxDeg, the whole CTA with
                        // its bitmap rows in global scratch
+  kTaskCtaRoot8 = 11,  // root b, split < d <= 256, the whole CTA, masks of up to 8 words in
+                       // registers
 };
 
 // Out-degree limits of the batched root tasks: the CTA bitmap of a root of out-degree d takes
