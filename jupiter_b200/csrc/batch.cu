@@ -147,27 +147,36 @@ __device__ __forceinline__ acc_t task_groups_k(const JobDesc& j, int64_t b, int6
   }
 }
 
+// The warps take the task's roots one at a time from a shared counter (zero at task start),
+// so a warp that drew cheap roots does not wait at the next task fetch for one that drew dear
+// ones.
 template <int K, bool PAIRS, bool TT = false>
 __device__ __forceinline__ acc_t warp_roots_k(const JobDesc& j, int64_t b, int64_t e,
-                                              WarpSmem& ws) {
+                                              WarpSmem& ws, int* next) {
+  const int lane = threadIdx.x & 31;
   acc_t cnt = 0, el = 0;
-  for (int64_t r = b + (threadIdx.x >> 5); r < e; r += 8)
+  for (;;) {
+    int q = 0;
+    if (lane == 0) q = atomicAdd(next, 1);
+    const int64_t r = b + __shfl_sync(kFull, q, 0);
+    if (r >= e) break;
     cnt += warp_root<K, false, PAIRS, PAIRS, TT>(j.drow, j.dcol, j.roots[r], ws, j.tri, el,
                                                  j.srow);
+  }
   return cnt;
 }
 
 __device__ __forceinline__ acc_t task_warp_roots(const JobDesc& j, int64_t b, int64_t e,
-                                                 WarpSmem& ws) {
-  if (j.kind == kJobDiamond) return warp_roots_k<3, true>(j, b, e, ws);
-  if (j.kind == kJobIndTT) return warp_roots_k<4, true, true>(j, b, e, ws);
+                                                 WarpSmem& ws, int* next) {
+  if (j.kind == kJobDiamond) return warp_roots_k<3, true>(j, b, e, ws, next);
+  if (j.kind == kJobIndTT) return warp_roots_k<4, true, true>(j, b, e, ws, next);
   switch (j.k) {
-    case 3: return warp_roots_k<3, false>(j, b, e, ws);
-    case 4: return warp_roots_k<4, false>(j, b, e, ws);
-    case 5: return warp_roots_k<5, false>(j, b, e, ws);
-    case 6: return warp_roots_k<6, false>(j, b, e, ws);
-    case 7: return warp_roots_k<7, false>(j, b, e, ws);
-    default: return warp_roots_k<8, false>(j, b, e, ws);
+    case 3: return warp_roots_k<3, false>(j, b, e, ws, next);
+    case 4: return warp_roots_k<4, false>(j, b, e, ws, next);
+    case 5: return warp_roots_k<5, false>(j, b, e, ws, next);
+    case 6: return warp_roots_k<6, false>(j, b, e, ws, next);
+    case 7: return warp_roots_k<7, false>(j, b, e, ws, next);
+    default: return warp_roots_k<8, false>(j, b, e, ws, next);
   }
 }
 
@@ -294,6 +303,7 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
   __shared__ uint32_t rows[256];
   __shared__ int degs[256];
   __shared__ unsigned long long s_task;
+  __shared__ int s_next;  // next root of a warp-roots task
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   int smem_kind = -1;  // which layout the dynamic shared memory holds (hash tables persist)
@@ -301,6 +311,8 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
     if (tid == 0) s_task = atomicAdd(&a.cursor[0], 1ull);
     __syncthreads();
     const int64_t ti = (int64_t)s_task;
+    // every warp has left the previous task here, so its root counter can start over
+    if (tid == 0) s_next = 0;
     __syncthreads();
     if (ti >= a.ntasks) break;
     const Task t = a.tasks[ti];
@@ -313,7 +325,7 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
       case kTaskGroup32: c = task_groups_k<32>(j, t.b, t.e, rows, degs); break;
       case kTaskWarpRoots:
         smem_kind = kTaskWarpRoots;
-        c = task_warp_roots(j, t.b, t.e, ws);
+        c = task_warp_roots(j, t.b, t.e, ws, &s_next);
         break;
       case kTaskCtaRoot:
         smem_kind = kTaskCtaRoot;
@@ -512,7 +524,7 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
       cta.push_back(make_task(job, r < cta16_end ? kTaskCtaRoot : kTaskCtaRoot8, r, r + 1));
     if (cta_end > large_end)
       o->dmax = std::max(o->dmax, std::min(g->max_out_degree, kBatchCtaMaxDeg));
-    add_range_tasks(warp, job, kTaskWarpRoots, cta_end, warp_end, std::max<int64_t>(8, rpt / 16));
+    add_range_tasks(warp, job, kTaskWarpRoots, cta_end, warp_end, std::max<int64_t>(8, rpt / 4));
     // lane groups for d <= 32
     struct Cut { int g; int64_t b, e; };
     const int64_t b16 = tu.min_group <= 16 ? t.deg_begin[16] : t.small_end;
