@@ -188,17 +188,22 @@ typedef struct {
 } jgpm_tuning;
 
 typedef struct {
-  double kernel_ms;       /* device time of the batch (task upload + kernel + count read-back) */
-  int32_t launches;       /* kernels launched: the persistent task kernel, plus a second
-                             persistent kernel for large 4-cycle apexes when there are any */
-  int32_t tasks;          /* tasks in the global queue */
+  double kernel_ms;       /* time of the batch on its stream, from before the host builds the
+                             task tables to the count read-back (task building and upload,
+                             kernels, read-back) */
+  int32_t launches;       /* kernels launched, one to three: the persistent task kernel, a
+                             light persistent kernel for the lane-group tasks, and one for the
+                             large 4-cycle apexes, each when it has work */
+  int32_t tasks;          /* tasks in the queues */
   jgpm_tuning used;
 } jgpm_batch_stats;
 
 /* Counts every job exactly in one persistent work-stealing launch: all jobs' work is cut into
- * tasks of one global queue that persistent CTAs drain; counts[i] receives job i's count.  The
- * large 4-cycle apexes of all jobs form a second queue, drained first, on the same stream, by a
- * second persistent kernel whose CTAs hold a shared-memory counter slab.
+ * tasks of one global queue that persistent CTAs drain; counts[i] receives job i's count.  Two
+ * kinds of task have queues and persistent kernels of their own, on the same stream: the large
+ * 4-cycle apexes of all jobs, drained first by CTAs that hold a shared-memory counter slab, and
+ * the lane-group roots (out-degree <= 32), drained last by a light kernel with more CTAs per
+ * SM.
  * Replaces, for a whole batch, the reference's per-query round loop and static chunking
  * (src/jupiter_gpm.cu:356-375).  tuning = NULL uses the defaults.  All graphs must be on one
  * device. */

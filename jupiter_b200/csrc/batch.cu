@@ -55,9 +55,9 @@ namespace jgpm {
 struct BatchArgs {
   const JobDesc* jobs;
   const Task* tasks;
-  int64_t ntasks;
+  int64_t nmain, ntasks;       // k_batch: tasks [0, nmain); k_batch_groups: [nmain, ntasks)
   unsigned long long* counts;
-  unsigned long long* cursor;  // [0] task queue
+  unsigned long long* cursor;  // [0] main queue, [1] large 4-cycle apexes, [2] lane groups
   int32_t* list_scratch;  // per warp: kLevels lists of list_cap ints
   int64_t list_cap;
   int dmax, W;            // CTA-root bitmap layout
@@ -300,8 +300,6 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
   WarpSmem& ws = reinterpret_cast<WarpSmem*>(smem)[threadIdx.x >> 5];
   C4WarpHash& hash = reinterpret_cast<C4WarpHash*>(smem)[threadIdx.x >> 5];
   C4MidSmem<256>& c4m = *reinterpret_cast<C4MidSmem<256>*>(smem);
-  __shared__ uint32_t rows[256];
-  __shared__ int degs[256];
   __shared__ unsigned long long s_task;
   __shared__ int s_next;  // next root of a warp-roots task
   const int tid = threadIdx.x;
@@ -314,15 +312,11 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
     // every warp has left the previous task here, so its root counter can start over
     if (tid == 0) s_next = 0;
     __syncthreads();
-    if (ti >= a.ntasks) break;
+    if (ti >= a.nmain) break;
     const Task t = a.tasks[ti];
     const JobDesc j = a.jobs[t.job];
     acc_t c = 0;
     switch (t.kind) {
-      case kTaskGroup4: c = task_groups_k<4>(j, t.b, t.e, rows, degs); break;
-      case kTaskGroup8: c = task_groups_k<8>(j, t.b, t.e, rows, degs); break;
-      case kTaskGroup16: c = task_groups_k<16>(j, t.b, t.e, rows, degs); break;
-      case kTaskGroup32: c = task_groups_k<32>(j, t.b, t.e, rows, degs); break;
       case kTaskWarpRoots:
         smem_kind = kTaskWarpRoots;
         c = task_warp_roots(j, t.b, t.e, ws, &s_next);
@@ -357,6 +351,35 @@ __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs a) {
         }
         for (int64_t q = t.b; q < t.e; ++q) c += c4_mid_apex<256>(j.rrow, j.rcol, j.mid[q], c4m);
         break;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+    if (lane == 0 && c) atomicAdd(&a.counts[t.job], c);
+  }
+}
+
+// Lane-group tasks (roots of out-degree <= 32) of every job, on a light kernel: no dynamic
+// shared memory and few registers, so that enough CTAs per SM hide the latency of these short
+// roots (k_batch, which holds every other task kind, runs four).  Launched after k_batch.
+__global__ void __launch_bounds__(256, 5) k_batch_groups(BatchArgs a) {
+  __shared__ uint32_t rows[256];
+  __shared__ int degs[256];
+  __shared__ unsigned long long s_task;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  for (;;) {
+    if (tid == 0) s_task = atomicAdd(&a.cursor[2], 1ull);
+    __syncthreads();
+    const int64_t ti = a.nmain + (int64_t)s_task;
+    __syncthreads();
+    if (ti >= a.ntasks) break;
+    const Task t = a.tasks[ti];
+    const JobDesc j = a.jobs[t.job];
+    acc_t c = 0;
+    switch (t.kind) {
+      case kTaskGroup4: c = task_groups_k<4>(j, t.b, t.e, rows, degs); break;
+      case kTaskGroup8: c = task_groups_k<8>(j, t.b, t.e, rows, degs); break;
+      case kTaskGroup16: c = task_groups_k<16>(j, t.b, t.e, rows, degs); break;
+      default: c = task_groups_k<32>(j, t.b, t.e, rows, degs); break;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
     if (lane == 0 && c) atomicAdd(&a.counts[t.job], c);
@@ -564,6 +587,7 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
     at += v.size();
   }
   c.h_tasks.n = total;
+  c.nmain = (int64_t)(total - light.size());  // lane-group tasks last: k_batch_groups
   c.tri_off.swap(tri_off);
   return JGPM_OK;
 }
@@ -590,7 +614,7 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   if ((rc = c.jobs.reserve(nj * sizeof(JobDesc)))) return rc;
   if ((rc = c.tasks.reserve(std::max<size_t>(1, nt) * sizeof(Task)))) return rc;
   if ((rc = c.counts.reserve(nj * sizeof(unsigned long long)))) return rc;
-  if ((rc = c.cursor.reserve(2 * sizeof(unsigned long long)))) return rc;
+  if ((rc = c.cursor.reserve(3 * sizeof(unsigned long long)))) return rc;
   if (o.tri_bytes) {
     if ((rc = c.tri.reserve(o.tri_bytes))) return rc;
     for (size_t ji = 0; ji < nj; ++ji)
@@ -618,7 +642,7 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
                                   cudaMemcpyHostToDevice, s));
   if ((rc = c.h_tasks.record(s))) return rc;
   JGPM_CUDA_TRY(cudaMemsetAsync(c.counts.p, 0, nj * sizeof(unsigned long long), s));
-  JGPM_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, 2 * sizeof(unsigned long long), s));
+  JGPM_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, 3 * sizeof(unsigned long long), s));
   // large 4-cycle apexes: k_batch_c4_large on the same stream, before k_batch.  (Run side by
   // side on two streams the two kernels took twice their sum: the persistent k_batch CTAs hold
   // the SMs whose shared memory the slab CTAs need, and the two working sets share L2.)
@@ -666,13 +690,22 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   a.dmax = o.dmax;
   a.W = W;
   a.intersect = tu.intersect;
-  if (nt) k_batch<<<grid, 256, smem, s>>>(a);
+  const int64_t nmain = c.nmain;
+  a.nmain = nmain;
+  if (nmain) k_batch<<<grid, 256, smem, s>>>(a);
+  int glaunch = 0;
+  if ((int64_t)nt > nmain) {
+    int gper = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&gper, k_batch_groups, 256, 0);
+    k_batch_groups<<<sms * std::max(1, gper), 256, 0, s>>>(a);
+    glaunch = 1;
+  }
   JGPM_CUDA_TRY(cudaGetLastError());
   if (h_counts)
     JGPM_CUDA_TRY(cudaMemcpyAsync(h_counts, c.counts.p, nj * sizeof(uint64_t),
                                   cudaMemcpyDeviceToHost, s));
   if (ntasks_out) *ntasks_out = (int)(nt + n4);
-  if (launches_out) *launches_out = (nt ? 1 : 0) + (n4 ? 1 : 0);
+  if (launches_out) *launches_out = (nmain ? 1 : 0) + glaunch + (n4 ? 1 : 0);
   return JGPM_OK;
 }
 

@@ -143,6 +143,7 @@ struct BatchCtx {
   PinnedTasks h_tasks;           // the main queue
   std::vector<Task> h_c4_tasks;  // large 4-cycle apexes, by job, heaviest first
   std::vector<Task> cls[6];      // per-class task lists while building (capacity kept)
+  int64_t nmain = 0;             // tasks of k_batch; the lane-group tasks follow them
   std::vector<size_t> tri_off;  // diamond jobs: offset of the job's counters in `tri`
   size_t c4_zeroed = 0;
   size_t c4_cap_bytes = (size_t)4 << 30;  // memory cap of the 4-cycle counter arrays

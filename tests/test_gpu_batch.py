@@ -52,7 +52,7 @@ def test_batch_matches_plain_and_oracle(gpu, mixed):
     specs, gs, want = mixed
     jobs = [(g, p) for g in gs for p in PATTERNS]
     counts, st = gpu.batch_count(jobs)
-    assert st["launches"] in (1, 2) and st["tasks"] > 0
+    assert st["launches"] in (1, 2, 3) and st["tasks"] > 0
     for (g, p), c in zip(jobs, counts):
         assert c == want[(gs.index(g), p)], (gs.index(g), p)
 
