@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(256, 5) k_batch_groups(BatchArgs a) {
 
 // Large 4-cycle apexes of every 4-cycle job of the batch, heaviest first, on CTAs of 1024
 // threads, launched before k_batch on the same stream.  Each CTA has a shared-memory slab of
-// `words` words (kC4SlabWords, which the classifier's dense flags assume); an apex flagged dense
+// `words` words (a slab form of NT threads); an apex flagged dense
 // counts in the CTA's dense array (and touched list) of `stride` ints instead when the batch
 // has them.
 struct C4BatchArgs {
@@ -406,13 +406,14 @@ struct C4BatchArgs {
 constexpr uint64_t kC4TaskWedges = 1u << 16;  // wedge bound of a run of light large apexes
 constexpr int64_t kC4MidPerTask = 16;
 
-__global__ void __launch_bounds__(kC4SlabThreads) k_batch_c4_large(C4BatchArgs a) {
+template <int NT>
+__global__ void __launch_bounds__(NT, NT <= 512 ? 2 : 1) k_batch_c4_large(C4BatchArgs a) {
   extern __shared__ __align__(16) uint32_t slab[];
-  __shared__ C4LargeSmem<kC4SlabThreads> sh;
+  __shared__ C4LargeSmem<NT> sh;
   __shared__ unsigned long long s_q[2];
   int32_t* dense = a.dense ? a.dense + (int64_t)blockIdx.x * a.stride : nullptr;
   vid_t* touched = a.dense ? a.touched + (int64_t)blockIdx.x * a.stride : nullptr;
-  c4_slab_zero<kC4SlabThreads>(slab, a.words);
+  c4_slab_zero<NT>(slab, a.words);
   if (threadIdx.x == 0) s_q[0] = atomicAdd(a.cursor, 1ull);
   __syncthreads();
   // double-buffered task fetch, as in the plain large-apex kernel: every task runs at least
@@ -429,9 +430,9 @@ __global__ void __launch_bounds__(kC4SlabThreads) k_batch_c4_large(C4BatchArgs a
       const uint32_t cw = (uint32_t)j.apexes[j.nlarge + p];
       const int cut = (int)(cw & ~kC4DenseFlag);
       if (!dense || !(cw & kC4DenseFlag))
-        c += c4_slab_apex<kC4SlabThreads>(j.rrow, j.rcol, v, cut, slab, a.words, sh);
+        c += c4_slab_apex<NT>(j.rrow, j.rcol, v, cut, slab, a.words, sh);
       else
-        c += c4_large_apex<kC4SlabThreads>(j.rrow, j.rcol, v, cut, dense, touched, sh);
+        c += c4_large_apex<NT>(j.rrow, j.rcol, v, cut, dense, touched, sh);
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(&a.counts[t.job], c);
@@ -462,6 +463,7 @@ struct BuildOut {
   int dmax = 33;          // largest CTA-root out-degree
   int wdmax = 0;          // largest wide-root out-degree (0: no wide roots)
   int64_t c4max = 0;      // largest vertex count of a job with dense-counted 4-cycle apexes
+  int64_t c4nmax = 0;     // largest vertex count of a job with large 4-cycle apexes
   int max_out = 0;        // largest out-degree among the large roots
   bool any_large = false;
   size_t tri_bytes = 0;   // diamond counters of the batch
@@ -507,6 +509,7 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
         c4w.push_back(w);
       }
       if (g->c4_ndense > 0) o->c4max = std::max<int64_t>(o->c4max, g->n);
+      if (g->c4_nlarge > 0) o->c4nmax = std::max<int64_t>(o->c4nmax, g->n);
       add_range_tasks(c4m, job, kTaskC4Mid, 0, g->c4_nmid, kC4MidPerTask);
       add_range_tasks(c4s, job, kTaskC4Small, 0, g->c4_nsmall, std::max<int64_t>(8, rpt / 8));
       c.h_jobs.push_back(jd);
@@ -648,11 +651,16 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   // the SMs whose shared memory the slab CTAs need, and the two working sets share L2.)
   const size_t n4 = c.h_c4_tasks.size();
   if (n4 > 0) {
-    const size_t slab_bytes = (size_t)kC4SlabWords * sizeof(uint32_t);
-    if ((rc = raise_smem_limit((const void*)k_batch_c4_large, slab_bytes))) return rc;
+    // the narrow slab form when every job with large apexes has at most kC4NarrowMaxN
+    // vertices (the form their dense flags assume); the wide form otherwise, which is exact
+    // for every apex too
+    const C4SlabForm form = c4_slab_form(o.c4nmax);
+    const size_t slab_bytes = (size_t)form.words * sizeof(uint32_t);
+    auto kern = form.threads == kC4NarrowThreads ? k_batch_c4_large<kC4NarrowThreads>
+                                                  : k_batch_c4_large<kC4WideThreads>;
+    if ((rc = raise_smem_limit((const void*)kern, slab_bytes))) return rc;
     int c4_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c4_per_sm, k_batch_c4_large, kC4SlabThreads,
-                                                  slab_bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c4_per_sm, kern, form.threads, slab_bytes);
     int64_t ctas = std::min<int64_t>((int64_t)sms * std::max(1, c4_per_sm), (int64_t)n4);
     const size_t per_cta = (size_t)o.c4max * sizeof(int32_t);  // 0: no dense apex
     if (per_cta) ctas = std::min<int64_t>(ctas, (int64_t)(c.c4_cap_bytes / per_cta));
@@ -678,8 +686,8 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     b.dense = need ? (int32_t*)c.c4.p : nullptr;
     b.touched = need ? (vid_t*)c.c4t.p : nullptr;
     b.stride = o.c4max;
-    b.words = kC4SlabWords;
-    k_batch_c4_large<<<(int)ctas, kC4SlabThreads, slab_bytes, s>>>(b);
+    b.words = form.words;
+    kern<<<(int)ctas, form.threads, slab_bytes, s>>>(b);
     JGPM_CUDA_TRY(cudaGetLastError());
   }
   a.jobs = (const JobDesc*)c.jobs.p;

@@ -50,7 +50,7 @@ __global__ void k_c4_classify(const eid_t* rp, const vid_t* col, vid_t n, vid_t*
       } else {
         const unsigned long long p = atomicAdd(&counters[1], 1ull);
         large_list[p] = (vid_t)v;
-        const bool dense = c4_dense_apex((vid_t)v, cut, ub, kC4SlabWords);
+        const bool dense = c4_dense_apex((vid_t)v, cut, ub, c4_slab_form(n));
         large_key[p] = ub | (dense ? 0ull : kC4SlabKey);
         if (dense) atomicAdd(&counters[3], 1ull);
       }
@@ -115,23 +115,23 @@ __global__ void __launch_bounds__(kC4MidThreads) k_c4_mid(const eid_t* rp, const
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
 }
 
-// Large apexes on CTAs of kC4SlabThreads (1024) threads, so that one slab (or one dense array)
-// is shared by as many warps as a CTA holds.  SLAB: every apex of the list counts in the CTA's
-// shared-memory slab of `words` words (one CTA per SM).  Otherwise every apex counts in the
-// CTA's dense array (counters: 2n ints per CTA, n counters then n touched ids), a lighter
-// kernel with two CTAs per SM.  cuts: the stored cut of each apex of the list.
-template <bool SLAB>
-__global__ void __launch_bounds__(kC4SlabThreads)
+// Large apexes on CTAs of NT threads.  SLAB: every apex of the list counts in the CTA's
+// shared-memory slab of `words` words (a slab form: 1024 threads and one CTA per SM, or 512
+// threads and two).  Otherwise every apex counts in the CTA's dense array (counters: 2n ints
+// per CTA, n counters then n touched ids), a lighter kernel with two 1024-thread CTAs per SM.
+// cuts: the stored cut of each apex of the list.
+template <int NT, bool SLAB>
+__global__ void __launch_bounds__(NT, (NT <= 512 || !SLAB) ? 2 : 1)
     k_c4_large(const eid_t* rp, const vid_t* col, vid_t n, const vid_t* list,
                const uint32_t* cuts, int64_t nlist, unsigned long long* cursor,
                int32_t* counters, int words, DevControl* ctl) {
   extern __shared__ __align__(16) uint32_t slab[];
   __shared__ unsigned long long s_q[2];
-  __shared__ C4LargeSmem<kC4SlabThreads> sh;
+  __shared__ C4LargeSmem<NT> sh;
   int32_t* dense = SLAB ? nullptr : counters + (int64_t)blockIdx.x * 2 * n;
   vid_t* touched = SLAB ? nullptr : dense + n;
   const int tid = threadIdx.x, lane = tid & 31;
-  if (SLAB) c4_slab_zero<kC4SlabThreads>(slab, words);
+  if (SLAB) c4_slab_zero<NT>(slab, words);
   if (tid == 0) s_q[0] = atomicAdd(cursor, 1ull);
   __syncthreads();
   acc_t sum = 0;
@@ -145,9 +145,9 @@ __global__ void __launch_bounds__(kC4SlabThreads)
     const vid_t v = list[q];
     const int cut = (int)(cuts[q] & ~kC4DenseFlag);
     if (SLAB)
-      sum += c4_slab_apex<kC4SlabThreads>(rp, col, v, cut, slab, words, sh);
+      sum += c4_slab_apex<NT>(rp, col, v, cut, slab, words, sh);
     else
-      sum += c4_large_apex<kC4SlabThreads>(rp, col, v, cut, dense, touched, sh);
+      sum += c4_large_apex<NT>(rp, col, v, cut, dense, touched, sh);
   }
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
   if (lane == 0 && sum) atomicAdd(&ctl->count[0], sum);
@@ -264,20 +264,22 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
   const int32_t n = g->n;
   const int sms = device_sm_count(g->device);
   const int64_t nsmall = g->c4_nsmall, nmid = g->c4_nmid, nlarge = g->c4_nlarge;
-  // Large apexes: the slab ones (first in the list) on one CTA per SM with a shared-memory slab,
-  // then the dense ones on two CTAs per SM with dense counters and touched lists (2n ints per
-  // CTA, within a 12 GiB cap).  The dense arrays are allocated for this count only (a graph
+  // Large apexes: the slab ones (first in the list) on CTAs with a shared-memory slab of the
+  // graph's slab form, then the dense ones on two CTAs per SM with dense counters and touched
+  // lists (2n ints per CTA, within a 12 GiB cap).  The dense arrays are allocated for this count only (a graph
   // pool would otherwise keep one such array set per graph), or taken from a small per-device
   // cache.
   const int64_t ndense = g->c4_ndense, nslab = nlarge - ndense;
   const uint32_t* cuts = (const uint32_t*)(g->d_c4_large + nlarge);
-  const size_t slab_bytes = (size_t)kC4SlabWords * sizeof(uint32_t);
+  const C4SlabForm form = c4_slab_form(n);
+  const size_t slab_bytes = (size_t)form.words * sizeof(uint32_t);
+  auto slab_kern = form.threads == kC4NarrowThreads ? k_c4_large<kC4NarrowThreads, true>
+                                                     : k_c4_large<kC4WideThreads, true>;
   int64_t slab_ctas = 0;
   if (nslab > 0) {
-    if ((rc = raise_smem_limit((const void*)k_c4_large<true>, slab_bytes))) return rc;
+    if ((rc = raise_smem_limit((const void*)slab_kern, slab_bytes))) return rc;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_large<true>, kC4SlabThreads,
-                                                  slab_bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, slab_kern, form.threads, slab_bytes);
     slab_ctas = std::min<int64_t>((int64_t)sms * std::max(1, per_sm), nslab);
   }
   const int64_t per_cta = (int64_t)n * 8;
@@ -335,14 +337,14 @@ int count_c4_wedge(jgpm_graph* g, uint64_t* out, double* ms) {
     g->launches += 1;
   }
   if (nslab > 0) {
-    k_c4_large<true><<<(int)slab_ctas, kC4SlabThreads, slab_bytes, s>>>(
+    slab_kern<<<(int)slab_ctas, form.threads, slab_bytes, s>>>(
         g->d_rank_rowptr, g->d_rank_col, n, g->d_c4_large, cuts, nslab, &g->d_ctl->counter[1],
-        nullptr, kC4SlabWords, g->d_ctl);
+        nullptr, form.words, g->d_ctl);
     g->launches += 1;
   }
   if (ndense > 0) {
     JGPM_CUDA_TRY(cudaMemsetAsync(dense, 0, dense_bytes, s));
-    k_c4_large<false><<<(int)ctas, kC4SlabThreads, 0, s>>>(
+    k_c4_large<kC4DenseThreads, false><<<(int)ctas, kC4DenseThreads, 0, s>>>(
         g->d_rank_rowptr, g->d_rank_col, n, g->d_c4_large + nslab, cuts + nslab, ndense,
         &g->d_ctl->counter[3], (int32_t*)dense, 0, g->d_ctl);
     g->launches += 1;

@@ -23,15 +23,30 @@ namespace jgpm {
 // Apex classes by their wedge upper bound ub (sum of deg(x) over the prefix):
 //   small  ub <= kC4SmallBound  one warp, shared-memory hash of kC4HashSlots (load <= 1/2);
 //   mid    ub <= kC4MidBound    one CTA, shared-memory hash of kC4MidSlots (load <= 1/2);
-//   large                       one CTA of 1024 threads, either a shared-memory slab of packed
-//                               counters swept over the vertex range in slices, or a dense
+//   large                       one CTA, either a shared-memory slab of packed counters swept
+//                               over the vertex range in slices (C4SlabForm), or a dense
 //                               counter array in global memory (c4_dense_apex).
 constexpr int kC4SmallBound = 256;
 constexpr int kC4HashSlots = 512;
 constexpr int kC4MidBound = 2048;
 constexpr int kC4MidSlots = 4096;
-constexpr int kC4SlabWords = 48 * 1024;  // 192 KB of 32-bit words
 constexpr int kC4MaxSlices = 4;
+
+// The two slab forms of the large apexes.  Wide: one CTA of 1024 threads per SM with a 192 KB
+// slab.  Narrow: two CTAs of 512 threads per SM with 96 KB each, so that one CTA's adds overlap
+// the other's latency-bound phases (the loads of x, rp[x] and the boundary searches between
+// barriers).  The narrow slab covers half the ids per slice, so a graph takes it only up to
+// kC4NarrowMaxN vertices, where an 8-bit apex still needs at most kC4MaxSlices slices.
+struct C4SlabForm {
+  int threads, words;
+};
+constexpr int kC4WideThreads = 1024, kC4WideWords = 48 * 1024;
+constexpr int kC4NarrowThreads = 512, kC4NarrowWords = 24 * 1024;
+constexpr int64_t kC4NarrowMaxN = (int64_t)kC4MaxSlices * (kC4NarrowWords << 2);  // 393,216
+__host__ __device__ __forceinline__ C4SlabForm c4_slab_form(int64_t n) {
+  return n <= kC4NarrowMaxN ? C4SlabForm{kC4NarrowThreads, kC4NarrowWords}
+                            : C4SlabForm{kC4WideThreads, kC4WideWords};
+}
 
 // Per-warp shared memory of the small-apex path.
 struct C4WarpHash {
@@ -82,20 +97,20 @@ __host__ __device__ __forceinline__ int64_t c4_slab_slices(vid_t v, int cut, int
   return ((int64_t)v + span - 1) / span;
 }
 
-// Threads of a large-apex CTA (slab and dense kernels, plain and batched).
-constexpr int kC4SlabThreads = 1024;
+// Threads of a dense-counter CTA (the plain dense kernel, two CTAs per SM).
+constexpr int kC4DenseThreads = 1024;
 
-// Whether a large apex counts in a dense global array rather than in the slab.  The slab costs
-// a layout and a boundary search per x for every (slice, block of kC4SlabThreads x), so an
-// apex takes it when it needs at most kC4MaxSlices slices or brings at least kC4SliceWedges of
-// wedge bound per (slice, block).  (Dense counters of a graph of millions of vertices do not
-// stay in L2: every wedge then costs an atomic in DRAM, about ten times a slab add.)  The
+// Whether a large apex counts in a dense global array rather than in the slab of form f.  The
+// slab costs a layout and a boundary search per x for every (slice, block of f.threads x), so
+// an apex takes it when it needs at most kC4MaxSlices slices or brings at least kC4SliceWedges
+// of wedge bound per (slice, block).  (Dense counters of a graph of millions of vertices do
+// not stay in L2: every wedge then costs an atomic in DRAM, about ten times a slab add.)  The
 // classifier decides with this one function and records it with the apex.
 constexpr uint64_t kC4SliceWedges = 1024;
 __host__ __device__ __forceinline__ bool c4_dense_apex(vid_t v, int cut, uint64_t ub,
-                                                       int words) {
-  const int64_t sl = c4_slab_slices(v, cut, words);
-  const int64_t nblk = ((int64_t)cut + kC4SlabThreads - 1) / kC4SlabThreads;
+                                                       C4SlabForm f) {
+  const int64_t sl = c4_slab_slices(v, cut, f.words);
+  const int64_t nblk = ((int64_t)cut + f.threads - 1) / f.threads;
   return sl > kC4MaxSlices && ub < (uint64_t)(sl * nblk) * kC4SliceWedges;
 }
 

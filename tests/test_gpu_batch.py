@@ -147,6 +147,11 @@ def test_batch_c4_slab_and_dense(gpu, mixed):
             counts, st = gpu.batch_count(jobs)
             assert counts == exp
             assert st["launches"] == 2
+            # without the 2^20 graph every large apex fits the narrow slab form (two CTAs of
+            # 512 threads per SM)
+            keep = [0, 2, 3, 4, 5, 6]
+            counts, _ = gpu.batch_count([jobs[i] for i in keep])
+            assert counts == [exp[i] for i in keep]
     finally:
         for g in big:
             g.close()
