@@ -39,13 +39,14 @@ constexpr int kC4MaxSlices = 4;
 // kC4NarrowMaxN vertices, where an 8-bit apex still needs at most kC4MaxSlices slices.
 struct C4SlabForm {
   int threads, words;
+  int slice_wedges;  // c4_dense_apex: wedge bound an apex must bring per (slice, block)
 };
 constexpr int kC4WideThreads = 1024, kC4WideWords = 48 * 1024;
 constexpr int kC4NarrowThreads = 512, kC4NarrowWords = 24 * 1024;
 constexpr int64_t kC4NarrowMaxN = (int64_t)kC4MaxSlices * (kC4NarrowWords << 2);  // 393,216
 __host__ __device__ __forceinline__ C4SlabForm c4_slab_form(int64_t n) {
-  return n <= kC4NarrowMaxN ? C4SlabForm{kC4NarrowThreads, kC4NarrowWords}
-                            : C4SlabForm{kC4WideThreads, kC4WideWords};
+  return n <= kC4NarrowMaxN ? C4SlabForm{kC4NarrowThreads, kC4NarrowWords, 1024}
+                            : C4SlabForm{kC4WideThreads, kC4WideWords, 8192};
 }
 
 // Per-warp shared memory of the small-apex path.
@@ -102,16 +103,17 @@ constexpr int kC4DenseThreads = 1024;
 
 // Whether a large apex counts in a dense global array rather than in the slab of form f.  The
 // slab costs a layout and a boundary search per x for every (slice, block of f.threads x), so
-// an apex takes it when it needs at most kC4MaxSlices slices or brings at least kC4SliceWedges
+// an apex takes it when it needs at most kC4MaxSlices slices or brings at least f.slice_wedges
 // of wedge bound per (slice, block).  (Dense counters of a graph of millions of vertices do
 // not stay in L2: every wedge then costs an atomic in DRAM, about ten times a slab add.)  The
-// classifier decides with this one function and records it with the apex.
-constexpr uint64_t kC4SliceWedges = 1024;
+// thresholds are measured: 1024 for the narrow form; 8192 for the wide one, which on an R-MAT
+// graph of 16.7 M vertices took the 4-cycle count from 9.7 s (1024) to 7.8 s (4096: 8.3 s,
+// 65536: 9.0 s).  The classifier decides with this one function and records it with the apex.
 __host__ __device__ __forceinline__ bool c4_dense_apex(vid_t v, int cut, uint64_t ub,
                                                        C4SlabForm f) {
   const int64_t sl = c4_slab_slices(v, cut, f.words);
   const int64_t nblk = ((int64_t)cut + f.threads - 1) / f.threads;
-  return sl > kC4MaxSlices && ub < (uint64_t)(sl * nblk) * kC4SliceWedges;
+  return sl > kC4MaxSlices && ub < (uint64_t)(sl * nblk) * (uint64_t)f.slice_wedges;
 }
 
 // Sort key of a large apex: its wedge bound, with kC4SlabKey set for slab apexes, so that a
@@ -131,6 +133,20 @@ __device__ __forceinline__ int c4_lower_bound(const vid_t* a, int n, vid_t key) 
     else hi = mid;
   }
   return lo;
+}
+
+// First index p in [lo, n) with a[p] >= key (n if none), for a cursor lo below which every
+// entry is < key: probes lo, lo+1, lo+3, lo+7, ... and then searches the last gap.  One load
+// when the answer is lo, as it is for most slices of an apex that needs many of them.
+__device__ __forceinline__ int c4_gallop(const vid_t* a, int lo, int n, vid_t key) {
+  int p = lo, q = lo, step = 1;
+  while (q < n && __ldg(a + q) < key) {
+    p = q + 1;
+    q += step;
+    step <<= 1;
+  }
+  const int e = q < n ? q : n;
+  return p + c4_lower_bound(a + p, e - p, key);
 }
 
 // Visits the wedges (v, x, v3) for x = prefix[c0 .. c0+32) of N(v) below v, flattened over
@@ -464,7 +480,7 @@ __device__ __forceinline__ acc_t c4_slab_apex(const eid_t* rp, const vid_t* col,
           start = xb + s0;
           len = s1 - s0;
         } else if (one) {
-          const int s1 = cur + c4_lower_bound(col + xb + cur, xd - cur, hi);
+          const int s1 = c4_gallop(col + xb, cur, xd, hi);
           start = xb + cur;
           len = s1 - cur;
           cur = s1;
