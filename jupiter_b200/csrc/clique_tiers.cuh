@@ -268,6 +268,12 @@ inline bool launch_failed(cudaError_t* err) {
 template <int K>
 constexpr int kBandRowWords(int w) { return K >= 7 ? 0 : w; }
 
+// Mask words counted from registers in the band of out-degree <= 1024 (rows of up to 32
+// words): k = 4 row-parallel, k = 5 over (row, bit) pairs, one 32-word mask per thread; the
+// warp-cooperative form (0) otherwise.
+template <int K>
+constexpr int kWideBandRowWords() { return K == 4 || K == 5 ? 32 : 0; }
+
 // One CTA-root band: bitmap layout for out-degree <= dmax, masks of up to ROWW words counted
 // from registers, wider ones with WPL words per lane; GR puts the rows in global scratch.
 template <int K, bool STATS, bool ETRI, bool PAIRS, int ROWW, int WPL = 1, bool GR = false,
@@ -311,7 +317,7 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     if (launch_failed(&err)) return -1;
   }
   if (!p.mid[0].empty()) {
-    launch_mid_band<K, STATS, ETRI, PAIRS, 0, 1, false, TT>(a, p.mid[0], 1,
+    launch_mid_band<K, STATS, ETRI, PAIRS, kWideBandRowWords<K>(), 1, false, TT>(a, p.mid[0], 1,
                                                             std::min(max_out, kMidMaxDeg),
                                               sms, s);
     ++n;
