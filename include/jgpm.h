@@ -149,6 +149,22 @@ int jgpm_count(jgpm_graph* g, const char* pattern, int induced, int chunk_size, 
 int jgpm_count_ex(jgpm_graph* g, const char* pattern, int induced, int chunk_size,
                   unsigned flags, uint64_t* out, jgpm_stats* st);
 
+/* Counts the embeddings rooted at a strided sample of root arcs: the CSR slots begin,
+ * begin + stride, ... below end (end < 0: all) of the CSR the pattern's nested-loop plan
+ * runs on -- the DAG for "triangle" (P0) and the cliques P13..P16 ("4-clique".."7-clique",
+ * "k-clique:<k>" with k <= 7), the symmetric CSR otherwise.  Every embedding is rooted at
+ * exactly one arc, so counts over disjoint samples add up, and begin = 0, end < 0, stride = 1
+ * gives jgpm_count's result.  Runs the literal plan kernel (JGPM_COUNT_FORCE_PLAN; with
+ * induced = 1 the set-difference enumeration), so it matches a CPU run of the same plans on
+ * the same sample root arc for root arc.  The slots of one vertex v, [rowptr[v],
+ * rowptr[v+1]), count the embeddings rooted at v.  Replaces the reference's per-round root
+ * slice estart/enumber (src/jupiter_gpm.cu:373-377), here with a stride so that a sample
+ * spreads over the whole graph.  Closed-form patterns ("tailed-triangle", "4-path",
+ * "3-star" with induced = 0) have no plan: JGPM_EPATTERN.  end past the last root arc:
+ * JGPM_EINVAL. */
+int jgpm_count_roots(jgpm_graph* g, const char* pattern, int induced, int64_t begin,
+                     int64_t end, int64_t stride, uint64_t* out, jgpm_stats* st);
+
 /* Allocation-free count.  No counterpart in the reference: it exists for callers that may
  * not allocate device memory while they count (a host whose own allocator holds the device,
  * or a latency-critical path that must not call cudaMalloc/cudaFree).  It calls no

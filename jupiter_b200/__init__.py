@@ -140,6 +140,8 @@ def lib():
                              ctypes.POINTER(_Stats)]
     L.jgpm_count_ex.argtypes = [G, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_uint,
                                 _PU64, ctypes.POINTER(_Stats)]
+    L.jgpm_count_roots.argtypes = [G, ctypes.c_char_p, ctypes.c_int, ctypes.c_int64,
+                                   ctypes.c_int64, ctypes.c_int64, _PU64, ctypes.POINTER(_Stats)]
     L.jgpm_census4.argtypes = [G, _PU64, ctypes.POINTER(_Stats)]
     L.jgpm_setop.argtypes = [ctypes.c_int, _P32, ctypes.c_int32, _P32, ctypes.c_int32,
                              ctypes.c_int32, ctypes.c_int32, _P32, _P32]
@@ -282,6 +284,18 @@ class Graph:
                                "kernel_ms": st.kernel_ms, "rounds": st.rounds,
                                "method": METHODS.get(st.method, st.method),
                                "launches": st.launches}
+        return out.value
+
+    def count_roots(self, pattern, begin=0, end=-1, stride=1, induced=False, details=False):
+        """Count of the embeddings rooted at root arcs begin, begin + stride, ... < end of the
+        plan's CSR (the literal nested-loop plan; end < 0 means all arcs)."""
+        out = ctypes.c_uint64()
+        st = _Stats()
+        _check(lib().jgpm_count_roots(self._h, pattern.encode(), int(bool(induced)), int(begin),
+                                      int(end), int(stride), ctypes.byref(out),
+                                      ctypes.byref(st)))
+        if details:
+            return out.value, {"kernel_ms": st.kernel_ms, "launches": st.launches}
         return out.value
 
     def census4(self):

@@ -406,6 +406,47 @@ int jgpm_count(jgpm_graph* g, const char* pattern, int induced, int chunk_size, 
   return jgpm_count_ex(g, pattern, induced, chunk_size, 0u, out, st);
 }
 
+int jgpm_count_roots(jgpm_graph* g, const char* pattern, int induced, int64_t begin,
+                     int64_t end, int64_t stride, uint64_t* out, jgpm_stats* st) {
+  if (!g || !pattern || !out) {
+    jgpm_set_error_("jgpm_count_roots: null argument");
+    return JGPM_EINVAL;
+  }
+  if (begin < 0 || stride < 1 || (end >= 0 && end < begin)) {
+    jgpm_set_error_("jgpm_count_roots: need 0 <= begin <= end (or end < 0) and stride >= 1");
+    return JGPM_EINVAL;
+  }
+  ScopedDevice sd(g->device);
+  const int id = literal_plan_id(pattern, induced);
+  if (id < 0) {
+    jgpm_set_error_(std::string("jgpm_count_roots: no nested-loop plan for '") + pattern + "'" +
+                    (induced ? " (vertex-induced)" : ""));
+    return JGPM_EPATTERN;
+  }
+  const int64_t m = plan_root_arcs(g, id);
+  if (m < 0) return JGPM_ECUDA;  // DAG build failed (message set)
+  if (end > m) {
+    jgpm_set_error_("jgpm_count_roots: end is past the last root arc (" + std::to_string(m) +
+                    ")");
+    return JGPM_EINVAL;
+  }
+  g->launches = 0;
+  uint64_t count = 0;
+  double ms = 0.0;
+  int rc = count_roots_impl(g, id, begin, end < 0 ? m : end, stride, &count, &ms);
+  if (rc) return rc;
+  *out = count;
+  if (st) {
+    memset(st, 0, sizeof(*st));
+    st->count = count;
+    st->kernel_ms = ms;
+    st->rounds = 1;
+    st->method = JGPM_METHOD_PLAN;
+    st->launches = g->launches;
+  }
+  return JGPM_OK;
+}
+
 int jgpm_census4(jgpm_graph* g, uint64_t out[6], jgpm_stats* st) {
   if (!g || !out) {
     jgpm_set_error_("jgpm_census4: null argument");

@@ -148,5 +148,10 @@ int count_plan_impl(jgpm_graph* g, int id, int chunk_size, unsigned flags, bool 
                     uint64_t* out, uint64_t* elements, double* ms, int* method);
 int plan_id_of(const std::string& name, int induced);
 bool plan_uses_dag(int plan_id);
+// literal plan over sampled root arcs (plans.cu)
+int literal_plan_id(const std::string& name, int induced);
+int count_roots_impl(jgpm_graph* g, int id, int64_t begin, int64_t end, int64_t stride,
+                     uint64_t* out, double* ms);
+int64_t plan_root_arcs(jgpm_graph* g, int id);  // CSR slots of the plan's graph (-1: error)
 int count_census4(jgpm_graph* g, uint64_t out[6], double* ms);
 }  // namespace jgpm

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -88,7 +89,9 @@ struct PlanArgs {
   const eid_t* rowptr;
   const vid_t* col;
   vid_t n;
+  // root arcs: the CSR slots slot_begin + i * slot_stride, 0 <= i < nsamp (< slot_end)
   int64_t slot_begin, slot_end;
+  int64_t slot_stride, nsamp;
   DevControl* ctl;
   int32_t* scratch;
   int64_t cap;  // entries per scratch list (4 lists per warp)
@@ -474,23 +477,30 @@ __global__ void __launch_bounds__(256) k_plan(PlanArgs a) {
   L.Z = L.Y + a.cap;
   acc_t lc = 0, uc = 0, el = 0;
   constexpr int kChunk = 4;
+  // owner of slot s among the vertices [lo, n): the last v with rowptr[v] <= s
+  auto owner = [&](int64_t lo, int64_t s) {
+    int64_t hi = a.n;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (a.rowptr[mid] <= s) lo = mid;
+      else hi = mid - 1;
+    }
+    return (vid_t)lo;
+  };
   for (;;) {
     unsigned long long c0 = 0;
     if (lane == 0) c0 = atomicAdd(&a.ctl->counter[0], (unsigned long long)kChunk);
     c0 = __shfl_sync(kFull, c0, 0);
-    const int64_t s0 = a.slot_begin + (int64_t)c0;
-    if (s0 >= a.slot_end) break;
-    const int64_t s1 = min(s0 + kChunk, a.slot_end);
-    // owner of slot s0
-    int64_t lo = 0, hi = a.n;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi + 1) >> 1;
-      if (a.rowptr[mid] <= s0) lo = mid;
-      else hi = mid - 1;
-    }
-    vid_t v0 = (vid_t)lo;
-    for (int64_t s = s0; s < s1; ++s) {
-      while (a.rowptr[v0 + 1] <= s) ++v0;
+    if ((int64_t)c0 >= a.nsamp) break;
+    const int64_t i1 = min((int64_t)c0 + kChunk, a.nsamp);
+    vid_t v0 = owner(0, a.slot_begin + (int64_t)c0 * a.slot_stride);
+    for (int64_t i = (int64_t)c0; i < i1; ++i) {
+      const int64_t s = a.slot_begin + i * a.slot_stride;
+      if (a.slot_stride == 1) {
+        while (a.rowptr[v0 + 1] <= s) ++v0;
+      } else {
+        v0 = owner(v0, s);
+      }
       const vid_t v1 = __ldg(a.col + s);
       uc += run_plan<P, STATS>(a, v0, v1, L, lc, el);
     }
@@ -638,9 +648,11 @@ int read_ctl(jgpm_graph* g) {
   return JGPM_OK;
 }
 
-// Runs the literal plan kernel over all root arcs (rounds = chunk_size).
+// Runs the literal plan kernel over the root arcs begin, begin + stride, ... < end of the
+// plan's CSR (end < 0: all of them), split into chunk_size rounds of consecutive samples.
 int run_literal(jgpm_graph* g, int id, int chunk_size, bool stats, uint64_t* out,
-                uint64_t* elements, double* ms) {
+                uint64_t* elements, double* ms, int64_t begin = 0, int64_t end = -1,
+                int64_t stride = 1) {
   int rc;
   const bool dag = plan_uses_dag(id);
   if (dag && (rc = ensure_dag(g))) return rc;
@@ -661,18 +673,26 @@ int run_literal(jgpm_graph* g, int id, int chunk_size, bool stats, uint64_t* out
   a.scratch = (int32_t*)g->d_scratch;
   a.cap = cap;
   const int64_t m = dag ? g->m_dag : g->m;
+  if (end < 0 || end > m) end = m;
+  if (begin < 0) begin = 0;
+  if (stride < 1) stride = 1;
+  const int64_t nsamp = end > begin ? (end - begin + stride - 1) / stride : 0;
   const int grid = (int)(warps / 8);
   const int rounds = chunk_size > 1 ? chunk_size : 1;
-  const int64_t per = (m + rounds - 1) / rounds;
+  const int64_t per = (nsamp + rounds - 1) / rounds;
+  a.slot_stride = stride;
+  a.slot_end = end;
   Timer t;
   JGPM_CUDA_TRY(cudaMemsetAsync(g->d_ctl, 0, sizeof(DevControl), g->stream));
   cudaEventRecord(t.a, g->stream);
   for (int r = 0; r < rounds; ++r) {
-    a.slot_begin = std::min(m, (int64_t)r * per);
-    a.slot_end = std::min(m, a.slot_begin + per);
+    const int64_t i0 = std::min(nsamp, (int64_t)r * per);
+    const int64_t i1 = std::min(nsamp, i0 + per);
+    a.slot_begin = begin + i0 * stride;
+    a.nsamp = i1 - i0;
     if (r > 0)
       JGPM_CUDA_TRY(cudaMemsetAsync(g->d_ctl->counter, 0, sizeof(g->d_ctl->counter), g->stream));
-    if (a.slot_end > a.slot_begin) {
+    if (a.nsamp > 0) {
       if ((rc = launch_plan(id, a, stats, grid, g->stream))) return rc;
       ++g->launches;
     }
@@ -902,6 +922,37 @@ int count_plan_impl(jgpm_graph* g, int id, int chunk_size, unsigned flags, bool 
   return JGPM_OK;
 }
 
+// Plan id of a pattern name for the literal plan kernel, or -1: the plan_id_of names plus the
+// clique aliases "triangle"/"3-clique" (P0 on the DAG), "4-clique".."7-clique" and
+// "k-clique:<k>" for 3 <= k <= 7.  Closed-form edge-induced counts have no plan (-1).
+int literal_plan_id(const std::string& p, int induced) {
+  int k = 0;
+  if (!induced) {
+    if (p == "triangle" || p == "3-clique") k = 3;
+    else if (p == "6-clique") k = 6;
+    else if (p == "7-clique") k = 7;
+    else if (p.rfind("k-clique:", 0) == 0) k = std::atoi(p.c_str() + 9);
+    if (k != 0) return k == 3 ? (int)kP0 : (k >= 4 && k <= 7) ? (int)kK4 + (k - 4) : -1;
+  }
+  const int id = plan_id_of(p, induced);
+  return id >= kNTailed ? -1 : id;
+}
+
+// The literal plan over a strided sample of root arcs (the reference's per-round root slice
+// estart/enumber, src/jupiter_gpm.cu:373-377, generalised with a stride).
+int count_roots_impl(jgpm_graph* g, int id, int64_t begin, int64_t end, int64_t stride,
+                     uint64_t* out, double* ms) {
+  return run_literal(g, id, 1, false, out, nullptr, ms, begin, end, stride);
+}
+
+int64_t plan_root_arcs(jgpm_graph* g, int id) {
+  if (plan_uses_dag(id)) {
+    if (ensure_dag(g)) return -1;
+    return g->m_dag;
+  }
+  return g->m;
+}
+
 }  // namespace jgpm
 
 // ============================================================================
@@ -1023,6 +1074,8 @@ extern "C" int jgpm_count_noalloc(jgpm_graph* g, const char* pattern, int induce
   a.cap = cap;
   a.slot_begin = 0;
   a.slot_end = dag ? g->m_dag : g->m;
+  a.slot_stride = 1;
+  a.nsamp = a.slot_end;
   // The arrays keep the previous call's contents: the work cursors and the result must start
   // at zero.  Calls that overlap on the GPU share these arrays and race.
   cudaError_t e = cudaMemsetAsync(d.ctl, 0, sizeof(DevControl), g->stream);
