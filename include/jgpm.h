@@ -176,7 +176,8 @@ int jgpm_count_roots(jgpm_graph* g, const char* pattern, int induced, int64_t be
  * (triangle, P13..P16) need the DAG already built (JGPM_EINVAL otherwise).  The count equals
  * jgpm_count's.  The static arrays are shared per device: calls that overlap on one device
  * race, so callers serialise them.  The first call on each device looks up the arrays'
- * addresses; make it before any stream capture begins. */
+ * addresses and keeps them for the life of the process; make it before any stream capture
+ * begins, and do not reset the device (cudaDeviceReset) between calls. */
 int jgpm_count_noalloc(jgpm_graph* g, const char* pattern, int induced, uint64_t* out);
 
 /* Vertex-induced census of the six connected 4-vertex graphlets, out[0..5] = 3-star,

@@ -100,10 +100,6 @@ int read_control(jgpm_graph* g, cudaStream_t s) {
   JGPM_CUDA_TRY(cudaMemcpyAsync(g->h_ctl, g->d_ctl, sizeof(DevControl), cudaMemcpyDeviceToHost,
                                 s));
   JGPM_CUDA_TRY(cudaStreamSynchronize(s));
-  if (g->h_ctl->error) {
-    jgpm_set_error_("device error word set by a counting kernel");
-    return g->h_ctl->error < 0 ? g->h_ctl->error : JGPM_ECUDA;
-  }
   return JGPM_OK;
 }
 

@@ -45,14 +45,13 @@ struct RootTiers {
 
 struct jgpm_graph_impl;
 
-// Per-launch device control block: work counters, results and the error word.
+// Per-launch device control block: work counters and results.  No kernel has an error to
+// report: capacities are sized on the host before each launch and no kernel waits.
 struct DevControl {
   unsigned long long counter[12]; // work-stealing cursors
   unsigned long long count[4];    // pattern results
   unsigned long long elements[4]; // set-op elements (stats launches)
-  int error;                      // JGPM_E* raised inside a kernel (0 = none)
-  int error_info;
-  int pad[6];
+  int pad[8];
 };
 
 std::string cuda_error_string(cudaError_t e);
@@ -153,5 +152,6 @@ int literal_plan_id(const std::string& name, int induced);
 int count_roots_impl(jgpm_graph* g, int id, int64_t begin, int64_t end, int64_t stride,
                      uint64_t* out, double* ms);
 int64_t plan_root_arcs(jgpm_graph* g, int id);  // CSR slots of the plan's graph (-1: error)
+uint64_t count_scratch_bytes(const jgpm_graph* g, const std::string& pattern, int induced);
 int count_census4(jgpm_graph* g, uint64_t out[6], double* ms);
 }  // namespace jgpm

@@ -648,6 +648,14 @@ int read_ctl(jgpm_graph* g) {
   return JGPM_OK;
 }
 
+// Warps of a literal plan launch: as many as fit a 2 GiB scratch budget of four lists of
+// maxd + 32 entries each, at most 8 CTAs of 8 warps per SM.
+int64_t literal_warps(int sms, int32_t maxd) {
+  const int64_t per_warp = 4 * ((int64_t)maxd + 32);
+  int64_t warps = std::min<int64_t>((int64_t)sms * 64, ((int64_t)2 << 30) / (per_warp * 4));
+  return std::max<int64_t>(8, warps - warps % 8);
+}
+
 // Runs the literal plan kernel over the root arcs begin, begin + stride, ... < end of the
 // plan's CSR (end < 0: all of them), split into chunk_size rounds of consecutive samples.
 int run_literal(jgpm_graph* g, int id, int chunk_size, bool stats, uint64_t* out,
@@ -657,13 +665,10 @@ int run_literal(jgpm_graph* g, int id, int chunk_size, bool stats, uint64_t* out
   const bool dag = plan_uses_dag(id);
   if (dag && (rc = ensure_dag(g))) return rc;
   if ((rc = ensure_control(g))) return rc;
-  const int sms = device_sm_count(g->device);
   const int32_t maxd = dag ? g->max_out_degree : g->max_degree;
   const int64_t cap = (int64_t)maxd + 32;
   const int64_t per_warp = 4 * cap;
-  // as many warps as fit a 2 GiB scratch budget, at most 8 CTAs of 8 warps per SM
-  int64_t warps = std::min<int64_t>((int64_t)sms * 64, ((int64_t)2 << 30) / (per_warp * 4));
-  warps = std::max<int64_t>(8, warps - warps % 8);
+  const int64_t warps = literal_warps(device_sm_count(g->device), maxd);
   if ((rc = ensure_scratch(g, (size_t)(warps * per_warp) * sizeof(int32_t)))) return rc;
   PlanArgs a{};
   a.rowptr = dag ? g->d_dag_rowptr : g->d_rowptr;
@@ -945,6 +950,30 @@ int count_roots_impl(jgpm_graph* g, int id, int64_t begin, int64_t end, int64_t 
   return run_literal(g, id, 1, false, out, nullptr, ms, begin, end, stride);
 }
 
+// Device scratch that a jgpm_count of `pattern` allocates on g beyond the graph itself (0 for
+// the methods that need none): the literal plan kernel's per-warp lists, or the clique
+// tiers' heavy-root lists and global bitmap rows.  Needs the DAG's maximum out-degree for
+// the DAG plans (0 until the DAG is built).
+uint64_t count_scratch_bytes(const jgpm_graph* g, const std::string& pattern, int induced) {
+  const int sms = device_sm_count(g->device);
+  const int id = plan_id_of(pattern, induced);
+  const bool literal = id == kP3 || id == kP4 || id == kP5 || id == kP6 || id == kP7 ||
+                       id == kP8 || id == kP9 || id == kP10 || id == kP11 || id == kP12 ||
+                       id == kVsgm;
+  if (literal) {
+    const int32_t maxd = g->max_degree;
+    return (uint64_t)literal_warps(sms, maxd) * 4 * ((uint64_t)maxd + 32) * 4;
+  }
+  const int k = literal_plan_id(pattern, induced) == kP0 ? 3
+              : (id >= kK4 && id <= kK7) ? 4 + (id - kK4) : 0;
+  if (k == 0 && pattern.rfind("k-clique:", 0) != 0) return 0;
+  uint64_t b = 0;
+  const int32_t mo = g->max_out_degree;
+  if (mo > kWideMaxDeg) b += (uint64_t)6 * ((uint64_t)mo + 32) * sms * 2 * 8 * 4;  // list tier
+  if (mo > kMidMaxDeg) b += (uint64_t)96 << 20;  // wide tier rows (kept within L2 size)
+  return b;
+}
+
 int64_t plan_root_arcs(jgpm_graph* g, int id) {
   if (plan_uses_dag(id)) {
     if (ensure_dag(g)) return -1;
@@ -986,7 +1015,8 @@ std::mutex g_noalloc_mu;
 // the first call there.  In host code the array names are host-side stand-ins, not device
 // addresses, so they are never handed to a kernel directly.  The look-up can initialise the
 // module on that device, so a caller that captures streams makes its first call on each
-// device before any capture begins.
+// device before any capture begins.  The addresses are kept for the life of the process: a
+// cudaDeviceReset between calls would leave them stale, and is not supported.
 int noalloc_setup(int device, NoAllocDevice* out) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   NoAllocDevice& d = g_noalloc_dev[device];
@@ -1082,6 +1112,7 @@ extern "C" int jgpm_count_noalloc(jgpm_graph* g, const char* pattern, int induce
   if (e == cudaSuccess && a.slot_end > 0) {
     rc = launch_plan(id, a, false, (int)(warps / 8), g->stream);
     e = cudaGetLastError();
+    if (rc == JGPM_OK && e == cudaSuccess) g->launches = 1;
   }
   unsigned long long cnt = 0;
   if (e == cudaSuccess && rc == JGPM_OK)

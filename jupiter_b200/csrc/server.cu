@@ -299,6 +299,7 @@ void plain_worker(jgpm_server* s) {
     pg.plain_busy = true;
     pg.last_use = ++s->use_clock;
     s->inflight_frontier += q->frontier;
+    s->st.peak_frontier_bytes = std::max<uint64_t>(s->st.peak_frontier_bytes, s->inflight_frontier);
     jgpm_graph* g = pg.g;
     lk.unlock();
     uint64_t cnt = 0;
@@ -503,6 +504,9 @@ int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, ui
       q->frontier += std::min<uint64_t>((uint64_t)12 << 30,
                                         (uint64_t)device_sm_count(s->cfg.device) * 2 *
                                             (uint64_t)g->n * 8);
+    // the literal plan kernel's per-warp lists (up to 2 GiB) or the clique tiers' scratch,
+    // allocated on the graph while the query runs
+    q->frontier += count_scratch_bytes(g, qp, q->induced);
   } else {
     estimate_frontier(s, g, q->kind, &q->fr_own, &q->fr_shared);
   }

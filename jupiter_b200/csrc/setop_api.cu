@@ -142,14 +142,27 @@ int jgpm_setop_batch(int op, const int32_t* a, const int64_t* a_off, const int32
   JGPM_CUDA_TRY(dbo.init(b_off, (size_t)nops + 1, s));
   JGPM_CUDA_TRY(dup.init(upper, (size_t)nops, s));
   JGPM_CUDA_TRY(dex.init(exclude, (size_t)nops, s));
+  // device buffers for host result arrays, freed on every return path
+  struct DeviceBuf {
+    int32_t* p = nullptr;
+    ~DeviceBuf() {
+      if (p) cudaFree(p);
+    }
+  } tmp_counts, tmp_out;
   int32_t* dcounts = counts;
   int32_t* dout = out;
   bool counts_host = !is_device_ptr(counts);
   bool out_host = mat && !is_device_ptr(out);
-  if (counts_host) JGPM_CUDA_TRY(cudaMalloc(&dcounts, nops * sizeof(int32_t)));
+  if (counts_host) {
+    JGPM_CUDA_TRY(cudaMalloc(&tmp_counts.p, nops * sizeof(int32_t)));
+    dcounts = tmp_counts.p;
+  }
   if (mat) {
     JGPM_CUDA_TRY(doo.init(out_off, (size_t)nops + 1, s));
-    if (out_host) JGPM_CUDA_TRY(cudaMalloc(&dout, std::max<int64_t>(1, ho[nops]) * 4));
+    if (out_host) {
+      JGPM_CUDA_TRY(cudaMalloc(&tmp_out.p, std::max<int64_t>(1, ho[nops]) * 4));
+      dout = tmp_out.p;
+    }
   }
   const int64_t blocks = std::min<int64_t>((nops + 7) / 8, 148 * 16);
   k_setop_batch<<<(int)std::max<int64_t>(1, blocks), 256, 0, s>>>(
@@ -161,8 +174,6 @@ int jgpm_setop_batch(int op, const int32_t* a, const int64_t* a_off, const int32
   if (e == cudaSuccess && out_host && ho[nops] > 0)
     e = cudaMemcpyAsync(out, dout, ho[nops] * 4, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (counts_host) cudaFree(dcounts);
-  if (out_host) cudaFree(dout);
   if (e != cudaSuccess) {
     jgpm_set_error_(std::string("jgpm_setop_batch: ") + cudaGetErrorString(e));
     return JGPM_ECUDA;

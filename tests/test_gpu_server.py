@@ -139,3 +139,32 @@ def test_plain_lane_patterns(gpu):
         with pytest.raises(gpu.JgpmError) as e:
             s.submit(ids[0], "induced:P7")
         assert e.value.code == -5
+
+
+def test_plain_lane_budget_covers_literal_plan_scratch(gpu):
+    """A literal-plan query (P3) on a graph with a hub allocates per-warp candidate lists of
+    the maximum degree (up to 2 GiB) while it runs.  Admission counts them: with a budget
+    that holds the graph but not those lists the query is refused, with room for them it runs
+    and the admitted frontier covers them."""
+    J = gpu
+    hub = 60000
+    src = np.concatenate([np.zeros(hub, np.int32), np.arange(1, hub, dtype=np.int32)])
+    dst = np.concatenate([np.arange(1, hub + 1, dtype=np.int32),
+                          np.arange(2, hub + 1, dtype=np.int32)])
+    lists = 2 << 30  # 2 GiB: the literal kernel's cap for a maximum degree of 60,000
+    tight = J.Server(memory_budget_bytes=1 << 30, max_inflight=1, max_batch=4)
+    with tight:
+        gid = tight.add_graph(J.Graph.from_edges(src, dst, hub + 1))
+        with pytest.raises(J.JgpmError) as e:
+            tight.submit(gid, "P3")
+        assert e.value.code == -11
+    roomy = J.Server(memory_budget_bytes=4 << 30, max_inflight=1, max_batch=4)
+    with roomy:
+        gid = roomy.add_graph(J.Graph.from_edges(src, dst, hub + 1))
+        resident = roomy.stats()["resident_bytes"]  # at admission (the lists come later)
+        c, _ = roomy.wait(roomy.submit(gid, "P3"))
+        sym = O.build_csr(hub + 1, src, dst)
+        assert c == O.count("P3", sym)[0]
+        st = roomy.stats()
+        assert st["peak_frontier_bytes"] >= lists
+        assert st["peak_frontier_bytes"] + resident <= 4 << 30
