@@ -36,6 +36,9 @@ __device__ __forceinline__ acc_t tt_deg(const eid_t* srow, vid_t v) {
 }
 
 constexpr int kRangeCut = 32;  // restrict a row to [L0, Ld-1] when longer than this
+// Rows of at least this many elements (after the range cut) are scanned by a whole warp, one
+// row at a time; shorter ones are flattened over the lanes.
+constexpr int kLongRow = 32;
 
 // Largest power of two <= n (0 for n <= 0).
 __device__ __forceinline__ int top_pow2(int n) { return n > 0 ? 1 << (31 - __clz(n)) : 0; }
@@ -208,7 +211,7 @@ __device__ __forceinline__ uint32_t ld_row(const uint32_t* p) {
 template <int D, int WPL, bool STATS, bool GR = false>
 struct DistCount {
   __device__ __forceinline__ static acc_t run(const uint32_t (&mw)[WPL], const uint32_t* R,
-                                              int W, const int* deg, acc_t& elems) {
+                                              int W, const int* deg, acc_t& elems, int S) {
     const int lane = threadIdx.x & 31;
     acc_t s = 0;
     int pm = 0;
@@ -233,14 +236,14 @@ struct DistCount {
           word &= word - 1;
           const int j = (q * 32 + lw) * 32 + b;
           if (STATS && lane == 0) elems += (acc_t)pm + (acc_t)deg[j];
-          const uint32_t* Rj = R + (size_t)j * W;
+          const uint32_t* Rj = R + (size_t)j * S;
           uint32_t nxt[WPL];
 #pragma unroll
           for (int r = 0; r < WPL; ++r) {
             const int w = r * 32 + lane;
             nxt[r] = w < W ? (mw[r] & ld_row<GR>(Rj + w)) : 0u;
           }
-          s += DistCount<D - 1, WPL, STATS, GR>::run(nxt, R, W, deg, elems);
+          s += DistCount<D - 1, WPL, STATS, GR>::run(nxt, R, W, deg, elems, S);
         }
       }
     }
@@ -251,7 +254,7 @@ struct DistCount {
 template <int WPL, bool STATS, bool GR>
 struct DistCount<0, WPL, STATS, GR> {
   __device__ __forceinline__ static acc_t run(const uint32_t (&mw)[WPL], const uint32_t*, int,
-                                              const int*, acc_t&) {
+                                              const int*, acc_t&, int) {
     acc_t s = 0;  // per-lane partial; summed at the end
 #pragma unroll
     for (int q = 0; q < WPL; ++q) s += (acc_t)__popc(mw[q]);
@@ -267,7 +270,7 @@ struct DistCount<0, WPL, STATS, GR> {
 template <int D, int WMAX, bool STATS>
 struct RowCount {
   __device__ static acc_t run(const uint32_t (&m)[WMAX], const uint32_t* R, int W,
-                              const int* deg, acc_t& elems) {
+                              const int* deg, acc_t& elems, int S) {
     acc_t s = 0;
     int pm = 0;
     if (STATS) {
@@ -285,10 +288,10 @@ struct RowCount {
       bits &= bits - 1;
       if (STATS) elems += (acc_t)pm + (acc_t)deg[j];
       uint32_t nxt[WMAX];
-      const uint32_t* Rj = R + (size_t)j * W;
+      const uint32_t* Rj = R + (size_t)j * S;
 #pragma unroll
       for (int q = 0; q < WMAX; ++q) nxt[q] = q < W ? (m[q] & Rj[q]) : 0u;
-      s += RowCount<D - 1, WMAX, STATS>::run(nxt, R, W, deg, elems);
+      s += RowCount<D - 1, WMAX, STATS>::run(nxt, R, W, deg, elems, S);
     }
   }
 };
@@ -296,7 +299,7 @@ struct RowCount {
 template <int WMAX, bool STATS>
 struct RowCount<0, WMAX, STATS> {
   __device__ __forceinline__ static acc_t run(const uint32_t (&m)[WMAX], const uint32_t*, int,
-                                              const int*, acc_t&) {
+                                              const int*, acc_t&, int) {
     acc_t s = 0;
 #pragma unroll
     for (int w = 0; w < WMAX; ++w) s += (acc_t)__popc(m[w]);
@@ -346,7 +349,11 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
       len = ub > lb ? ub - lb : 0;
     }
     ws.rs[i] = s;
-    ws.off[i] = len;
+    // rows of kLongRow or more elements are scanned row by row below (deg[] then holds the
+    // cut length; the accounting pass needs the full one and scans every row flattened)
+    const bool lng = !STATS && len >= kLongRow;
+    if (!STATS) ws.deg[i] = len;
+    ws.off[i] = lng ? 0 : len;
   }
   __syncwarp();
   {  // exclusive scan: lane takes rows [4 lane, 4 lane + 4)
@@ -382,6 +389,24 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
       }
     }
   };
+  // long rows: the warp scans one row at a time, two elements per lane and iteration, so no
+  // element searches for its row
+  if (!STATS) {
+    for (int i = 0; i < d; ++i) {
+      const int len = ws.deg[i];
+      if (len < kLongRow) continue;
+      const eid_t rsi = ws.rs[i];
+      for (int t0 = lane; t0 < len; t0 += 64) {
+        const bool two = t0 + 32 < len;
+        const int t1 = two ? t0 + 32 : t0;
+        const vid_t x0 = __ldg(col + rsi + t0), x1 = __ldg(col + rsi + t1);
+        int p0, p1;
+        count_below2(ws.L, d, topL, x0, x1, p0, p1);
+        hit(i, p0, x0, rsi + t0);
+        if (two) hit(i, p1, x1, rsi + t1);
+      }
+    }
+  }
   // two scanned elements per lane and iteration; row i of element t = last i with off[i] <= t
   for (int t0 = lane; t0 < T; t0 += 64) {
     const bool two = t0 + 32 < T;
@@ -433,7 +458,8 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
 #pragma unroll
       for (int q = 0; q < kWarpW; ++q) m2[q] = q < w_d ? (Ri[q] & Rj[q]) : 0u;
       if (STATS) elems += (acc_t)(ws.off[i + 1] - ws.off[i]) + (acc_t)ws.deg[j];
-      cnt += RowCount<(K >= 5 ? K - 4 : 1), kWarpW, STATS>::run(m2, ws.R, w_d, ws.deg, elems);
+      cnt += RowCount<(K >= 5 ? K - 4 : 1), kWarpW, STATS>::run(m2, ws.R, w_d, ws.deg, elems,
+                                                                  w_d);
     }
     __syncwarp();
     return cnt;
@@ -442,7 +468,8 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
     uint32_t m[kWarpW];
 #pragma unroll
     for (int q = 0; q < kWarpW; ++q) m[q] = q < w_d ? ws.R[i * w_d + q] : 0u;
-    if (!PAIRS || TT) cnt += RowCount<K - 3, kWarpW, STATS>::run(m, ws.R, w_d, ws.deg, elems);
+    if (!PAIRS || TT)
+      cnt += RowCount<K - 3, kWarpW, STATS>::run(m, ws.R, w_d, ws.deg, elems, w_d);
     if (ETRI) {
       unsigned pc = 0;
 #pragma unroll
@@ -463,15 +490,33 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
   return PAIRS ? pairs : cnt;
 }
 
+// Row stride in words of a root with w_d-word rows: odd in shared memory, so that the rows
+// that the threads of a warp read at the same word index fall into different banks; rows in
+// global memory (GR) are packed.
+__host__ __device__ __forceinline__ int row_stride(int w_d, bool global_rows) {
+  return global_rows ? w_d : (w_d | 1);
+}
+
+// Balanced 5-clique count (BAL): per warp, the R_i & R_j masks of 32 (i, j) pairs (RW words
+// each, word q of lane l at q * 32 + l) and a list of kBalCap packed items (k | lane << 10).
+constexpr int kBalCap = 512;
+__host__ __device__ __forceinline__ size_t bal_bytes(int rw) {
+  return rw > 0 ? (size_t)8 * ((size_t)rw * 32 * 4 + (size_t)kBalCap * 2) : 0;
+}
+
 // Shared layout for one mid-tier root (dynamic shared memory):
 //   L[dmax] ids | off[dmax+1] exclusive row offsets | rs[dmax] row starts (int64) |
-//   deg[dmax] | R[dmax * W] rows | 8 warp sums
+//   deg[dmax] | ln[dmax] row lengths | R[dmax * row_stride(W)] rows | 8 warp sums |
+//   balanced-count buffers (bal_rw)
 struct MidLayout {
   int dmax, W;
-  __host__ __device__ size_t bytes() const { return bytes_no_rows() + (size_t)dmax * W * 4; }
+  int bal_rw = 0;  // mask words of the balanced 5-clique buffers (0: none)
+  __host__ __device__ size_t bytes() const {
+    return bytes_no_rows() + (size_t)dmax * row_stride(W, false) * 4;
+  }
   __host__ __device__ size_t bytes_no_rows() const {
-    return (size_t)dmax * 4 + (size_t)(dmax + 1) * 4 + (size_t)dmax * 8 + (size_t)dmax * 4 +
-           64 + 64;
+    return (size_t)dmax * 4 + (size_t)(dmax + 1) * 4 + (size_t)dmax * 8 + (size_t)dmax * 8 +
+           64 + 64 + bal_bytes(bal_rw) + (bal_rw > 0 ? 16 : 0);
   }
 };
 
@@ -480,27 +525,34 @@ struct MidSmem {
   int* off;
   eid_t* rs;
   int* deg;
+  int* ln;  // row lengths after the range cut
   uint32_t* R;
   int* wsum;
+  uint32_t* bal_m;     // balanced count: 8 warps x RW x 32 mask words
+  uint16_t* bal_list;  // balanced count: 8 warps x kBalCap items
   // rows = nullptr: the rows follow in shared memory (MidLayout); otherwise they live at
   // rows (dmax * W words of global scratch for this CTA) and shared memory holds the rest
   // (MidLayout::bytes_no_rows).
   __device__ __forceinline__ static MidSmem carve(unsigned char* smem, int dmax, int W,
-                                                  uint32_t* rows = nullptr) {
+                                                  uint32_t* rows = nullptr, int bal_rw = 0) {
     MidSmem m;
     m.L = reinterpret_cast<vid_t*>(smem);
     m.off = reinterpret_cast<int*>(m.L + dmax);
     m.rs = reinterpret_cast<eid_t*>(
         (reinterpret_cast<uintptr_t>(m.off + dmax + 1) + 7) & ~uintptr_t(7));
     m.deg = reinterpret_cast<int*>(m.rs + dmax);
-    uint32_t* after = reinterpret_cast<uint32_t*>(m.deg + dmax);
+    m.ln = m.deg + dmax;
+    uint32_t* after = reinterpret_cast<uint32_t*>(m.ln + dmax);
     if (rows) {
       m.R = rows;
       m.wsum = reinterpret_cast<int*>(after);
     } else {
       m.R = after;
-      m.wsum = reinterpret_cast<int*>(m.R + (size_t)dmax * W);
+      m.wsum = reinterpret_cast<int*>(m.R + (size_t)dmax * row_stride(W, false));
     }
+    m.bal_m = reinterpret_cast<uint32_t*>(
+        (reinterpret_cast<uintptr_t>(m.wsum + 8) + 15) & ~uintptr_t(15));
+    m.bal_list = reinterpret_cast<uint16_t*>(m.bal_m + (size_t)8 * bal_rw * 32);
     return m;
   }
 };
@@ -508,16 +560,158 @@ struct MidSmem {
 // Rows up to this many words (out-degree <= 512) are counted row-parallel from registers.
 constexpr int kCtaRowWords = 16;
 
+// Exclusive scan of off[0..d) in place over the CTA (blocked per thread, then across
+// warps); off[d] receives the total.
+__device__ __forceinline__ void cta_exclusive_scan(int* off, int d, int* wsum) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nthreads = blockDim.x;
+  const int per = (d + nthreads - 1) / nthreads;
+  const int b0 = min(d, tid * per), b1 = min(d, b0 + per);
+  int local = 0;
+  for (int i = b0; i < b1; ++i) local += off[i];
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  int wbase = 0;
+  for (int w = 0; w < warp; ++w) wbase += wsum[w];
+  int run = wbase + incl - local;
+  __syncthreads();
+  for (int i = b0; i < b1; ++i) {
+    const int l = off[i];
+    off[i] = run;
+    run += l;
+  }
+  if (tid == nthreads - 1) off[d] = run;
+  __syncthreads();
+}
+
+// Items t = lane, lane + 32, ... < nit of a balanced round: popc(M_owner & R_k) over the
+// first W words (W a compile-time multiple of 4 >= w_d; the mask words past w_d are zero).
+template <int W>
+__device__ __forceinline__ acc_t bal_items_w(const uint16_t* Lw, int nit, const uint32_t* Mw,
+                                             const uint32_t* R, int S) {
+  acc_t cnt = 0;
+  for (int t2 = threadIdx.x & 31; t2 < nit; t2 += 32) {
+    const uint32_t v = Lw[t2];
+    const uint32_t* Rk = R + (size_t)(v & 1023u) * S;
+    const uint32_t* Mo = Mw + (v >> 10);
+    int s = 0;
+#pragma unroll
+    for (int q = 0; q < W; ++q) s += __popc(Mo[q * 32] & Rk[q]);
+    cnt += (acc_t)s;
+  }
+  return cnt;
+}
+
+template <int RW>
+__device__ __forceinline__ acc_t bal_items(const uint16_t* Lw, int nit, const uint32_t* Mw,
+                                           const uint32_t* R, int S, int w_d) {
+  switch ((w_d + 3) >> 2) {
+    case 1: return bal_items_w<4>(Lw, nit, Mw, R, S);
+    case 2: return bal_items_w<(RW >= 8 ? 8 : 4)>(Lw, nit, Mw, R, S);
+    case 3: return bal_items_w<(RW >= 12 ? 12 : 4)>(Lw, nit, Mw, R, S);
+    case 4: return bal_items_w<(RW >= 16 ? 16 : 4)>(Lw, nit, Mw, R, S);
+    case 5: return bal_items_w<(RW >= 20 ? 20 : 4)>(Lw, nit, Mw, R, S);
+    case 6: return bal_items_w<(RW >= 24 ? 24 : 4)>(Lw, nit, Mw, R, S);
+    case 7: return bal_items_w<(RW >= 28 ? 28 : 4)>(Lw, nit, Mw, R, S);
+    default: return bal_items_w<(RW >= 32 ? 32 : 4)>(Lw, nit, Mw, R, S);
+  }
+}
+
+// 5-cliques of one root from its bitmap rows, with the work spread evenly over the lanes.
+// off[0..d] holds the exclusive prefix of the row popcounts (P = off[d] pairs (i, j), j a
+// bit of R_i).  A warp takes 32 pairs at a time: each lane forms m = R_i & R_j, then the
+// bits k of all 32 masks are expanded into an item list (at most kBalCap per round) that
+// the lanes take round-robin; an item adds popc(m & R_k).  The work per item is the same
+// for every lane, whatever the masks' sizes.
+template <int RW>
+__device__ __forceinline__ acc_t bal_count5(const int* off, int d, int topO,
+                                            const uint32_t* R, int w_d, int S,
+                                            uint32_t* Mw, uint16_t* Lw) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int P = off[d];
+  acc_t cnt = 0;
+  for (int base = warp * 32; base < P; base += nwarps * 32) {
+    const int p = base + lane;
+    uint32_t m2[RW];
+    int c = 0;
+    if (p < P) {
+      int i, i2;
+      count_below2(off + 1, d - 1, topO, p + 1, p + 1, i, i2);
+      const uint32_t* Ri = R + (size_t)i * S;
+      const int j = select_bit(Ri, w_d, p - off[i]);
+      const uint32_t* Rj = R + (size_t)j * S;
+#pragma unroll
+      for (int q = 0; q < RW; ++q) {
+        m2[q] = q < w_d ? (Ri[q] & Rj[q]) : 0u;
+        c += __popc(m2[q]);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < RW; ++q) m2[q] = 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < RW; ++q)
+      if (q < ((w_d + 3) & ~3)) Mw[q * 32 + lane] = m2[q];  // m2[q] = 0 for q >= w_d
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int first = incl - c;
+    const int C = __shfl_sync(kFull, incl, 31);
+    for (int r0 = 0; r0 < C; r0 += kBalCap) {
+      // this lane's items with index in [r0, r0 + kBalCap)
+      const int tend = min(first + c, r0 + kBalCap);
+      int t = first;
+      if (t < tend) {
+#pragma unroll
+        for (int q = 0; q < RW; ++q) {
+          uint32_t w = m2[q];
+          const int pc = __popc(w);
+          if (t + pc <= r0) {  // the whole word lies before this round
+            t += pc;
+            continue;
+          }
+          while (w != 0u && t < tend) {
+            const int b = __ffs(w) - 1;
+            w &= w - 1;
+            if (t >= r0) Lw[t - r0] = (uint16_t)((q * 32 + b) | (lane << 10));
+            ++t;
+          }
+        }
+      }
+      __syncwarp();
+      const int nit = min(C - r0, kBalCap);
+      cnt += bal_items<RW>(Lw, nit, Mw, R, S, w_d);
+      __syncwarp();
+    }
+  }
+  return cnt;
+}
+
 // One root of out-degree 32 < d <= dmax processed by the whole CTA (blockDim = 256).
 // Every thread calls it; returns this thread's partial count.  Rows of up to ROWW words are
 // counted row-parallel from registers, wider ones (or all, with ROWW = 0) warp-cooperatively
-// with WPL mask words per lane (rows of up to 32 WPL words).
+// with WPL mask words per lane (rows of up to 32 WPL words).  BAL (k = 5, rows of up to ROWW
+// words in shared memory, no accounting) counts with bal_count5; the layout then carries the
+// balanced-count buffers (MidLayout::bal_rw = ROWW).
 template <int K, bool STATS, bool ETRI, bool PAIRS = false, int ROWW = kCtaRowWords,
-          int WPL = 1, bool GR = false, bool TT = false>
+          int WPL = 1, bool GR = false, bool TT = false, bool BAL = false>
 __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
                                           const vid_t* __restrict__ col, vid_t u,
                                           const MidSmem& sm, uint32_t* tri, acc_t& elems,
                                           const eid_t* srow = nullptr) {
+  static_assert(!BAL || (K == 5 && !STATS && !ETRI && !GR && ROWW > 0),
+                "the balanced count is for plain 5-clique counts with rows in shared memory");
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
@@ -531,9 +725,10 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
   const eid_t base = rowptr[u];
   const int d = (int)(rowptr[u + 1] - base);
   const int w_d = (d + 31) >> 5;
+  const int S = row_stride(w_d, GR);
   for (int j = tid; j < d; j += nthreads) L[j] = __ldg(col + base + j);
   // global rows are built by L2 atomics and read at L2: clear them at L2 as well
-  for (int q = tid; q < d * w_d; q += nthreads) {
+  for (int q = tid; q < d * S; q += nthreads) {
     if (GR) __stcg(R + q, 0u);
     else R[q] = 0u;
   }
@@ -551,40 +746,19 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
       len = ub > lb ? ub - lb : 0;
     }
     rs[i] = s;
-    off[i] = len;
+    sm.ln[i] = len;
+    // rows of kLongRow or more elements are scanned row by row below; the accounting pass
+    // scans every row flattened
+    off[i] = (!STATS && len >= kLongRow) ? 0 : len;
   }
   __syncthreads();
-  {  // exclusive scan of off[0..d): blocked per thread, then across warps
-    const int per = (d + nthreads - 1) / nthreads;
-    const int b0 = min(d, tid * per), b1 = min(d, b0 + per);
-    int local = 0;
-    for (int i = b0; i < b1; ++i) local += off[i];
-    int incl = local;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) sm.wsum[warp] = incl;
-    __syncthreads();
-    int wbase = 0;
-    for (int w = 0; w < warp; ++w) wbase += sm.wsum[w];
-    int run = wbase + incl - local;
-    __syncthreads();
-    for (int i = b0; i < b1; ++i) {
-      const int l = off[i];
-      off[i] = run;
-      run += l;
-    }
-    if (tid == nthreads - 1) off[d] = run;
-    __syncthreads();
-  }
+  cta_exclusive_scan(off, d, sm.wsum);
   const int T = off[d];
   acc_t pairs = 0, tt = 0;
   const int topL = top_pow2(d), topO = top_pow2(d - 1);
   auto hit = [&](int i, int p, vid_t x, eid_t e) {
     if (p < d && L[p] == x) {
-      atomicOr(&R[(size_t)i * w_d + (p >> 5)], 1u << (p & 31));
+      atomicOr(&R[(size_t)i * S + (p >> 5)], 1u << (p & 31));
       if (ETRI) {
         const unsigned o = atomicAdd(tri + e, 1u);
         if (PAIRS) pairs += (acc_t)o;
@@ -592,8 +766,26 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
       }
     }
   };
-  // two scanned elements per thread and iteration; row i of element t = last i with
-  // off[i] <= t
+  // long rows: one warp per row, two elements per lane and iteration, so no element
+  // searches for its row
+  if (!STATS) {
+    for (int i = warp; i < d; i += nwarps) {
+      const int len = sm.ln[i];
+      if (len < kLongRow) continue;
+      const eid_t rsi = rs[i];
+      for (int t0 = lane; t0 < len; t0 += 64) {
+        const bool two = t0 + 32 < len;
+        const int t1 = two ? t0 + 32 : t0;
+        const vid_t x0 = __ldg(col + rsi + t0), x1 = __ldg(col + rsi + t1);
+        int p0, p1;
+        count_below2(L, d, topL, x0, x1, p0, p1);
+        hit(i, p0, x0, rsi + t0);
+        if (two) hit(i, p1, x1, rsi + t1);
+      }
+    }
+  }
+  // short rows: two scanned elements per thread and iteration; row i of element t = last i
+  // with off[i] <= t
   for (int t0 = tid; t0 < T; t0 += 2 * nthreads) {
     const bool two = t0 + nthreads < T;
     const int t1 = two ? t0 + nthreads : t0;
@@ -610,7 +802,7 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
   if (ETRI) {  // the root's own arcs: popc(R_i) + (rows with bit i) triangles each
     for (int i = tid; i < d; i += nthreads) {
       unsigned pc = 0;
-      for (int q = 0; q < w_d; ++q) pc += (unsigned)__popc(ld_row<GR>(R + (size_t)i * w_d + q));
+      for (int q = 0; q < w_d; ++q) pc += (unsigned)__popc(ld_row<GR>(R + (size_t)i * S + q));
       const unsigned tu = pc + (unsigned)deg[i];
       if (tu) {
         const unsigned o = atomicAdd(tri + base + i, tu);
@@ -634,55 +826,36 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
     // pairs, so one dense row does not hold up the CTA.  off[i] = pairs before row i.
     for (int i = tid; i < d; i += nthreads) {
       int c = 0;
-      for (int q = 0; q < w_d; ++q) c += __popc(R[(size_t)i * w_d + q]);
+      for (int q = 0; q < w_d; ++q) c += __popc(R[(size_t)i * S + q]);
       off[i] = c;
     }
     __syncthreads();
-    {  // exclusive scan of off[0..d): blocked per thread, then across warps
-      const int per = (d + nthreads - 1) / nthreads;
-      const int b0 = min(d, tid * per), b1 = min(d, b0 + per);
-      int local = 0;
-      for (int i = b0; i < b1; ++i) local += off[i];
-      int incl = local;
+    cta_exclusive_scan(off, d, sm.wsum);
+    if (BAL) {
+      cnt += bal_count5<RW>(off, d, topO, R, w_d, S, sm.bal_m + (size_t)warp * RW * 32,
+                            sm.bal_list + (size_t)warp * kBalCap);
+    } else {
+      const int P = off[d];
+      for (int p = tid; p < P; p += nthreads) {
+        int i, i2;
+        count_below2(off + 1, d - 1, topO, p + 1, p + 1, i, i2);
+        const uint32_t* Ri = R + (size_t)i * S;
+        const int j = select_bit(Ri, w_d, p - off[i]);
+        const uint32_t* Rj = R + (size_t)j * S;
+        uint32_t m2[RW];
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t;
+        for (int q = 0; q < RW; ++q) m2[q] = q < w_d ? (Ri[q] & Rj[q]) : 0u;
+        if (STATS) elems += (acc_t)(off[i + 1] - off[i]) + (acc_t)deg[j];
+        cnt += RowCount<(K >= 5 ? K - 4 : 1), RW, STATS>::run(m2, R, w_d, deg, elems, S);
       }
-      if (lane == 31) sm.wsum[warp] = incl;
-      __syncthreads();
-      int wbase = 0;
-      for (int w = 0; w < warp; ++w) wbase += sm.wsum[w];
-      int run = wbase + incl - local;
-      __syncthreads();
-      for (int i = b0; i < b1; ++i) {
-        const int l = off[i];
-        off[i] = run;
-        run += l;
-      }
-      if (tid == nthreads - 1) off[d] = run;
-      __syncthreads();
-    }
-    const int P = off[d];
-    for (int p = tid; p < P; p += nthreads) {
-      int i, i2;
-      count_below2(off + 1, d - 1, topO, p + 1, p + 1, i, i2);
-      const uint32_t* Ri = R + (size_t)i * w_d;
-      const int j = select_bit(Ri, w_d, p - off[i]);
-      const uint32_t* Rj = R + (size_t)j * w_d;
-      uint32_t m2[RW];
-#pragma unroll
-      for (int q = 0; q < RW; ++q) m2[q] = q < w_d ? (Ri[q] & Rj[q]) : 0u;
-      if (STATS) elems += (acc_t)(off[i + 1] - off[i]) + (acc_t)deg[j];
-      cnt += RowCount<(K >= 5 ? K - 4 : 1), RW, STATS>::run(m2, R, w_d, deg, elems);
     }
   } else if (ROWW > 0 && w_d <= ROWW) {
     // row-parallel: each thread owns rows, masks in registers
     for (int i = tid; i < d; i += nthreads) {
       uint32_t m[RW];
 #pragma unroll
-      for (int q = 0; q < RW; ++q) m[q] = q < w_d ? R[(size_t)i * w_d + q] : 0u;
-      cnt += RowCount<K - 3, RW, STATS>::run(m, R, w_d, deg, elems);
+      for (int q = 0; q < RW; ++q) m[q] = q < w_d ? R[(size_t)i * S + q] : 0u;
+      cnt += RowCount<K - 3, RW, STATS>::run(m, R, w_d, deg, elems, S);
     }
   } else {
     // wide rows: the mask is distributed over the lanes, WPL words each
@@ -691,9 +864,9 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
 #pragma unroll
       for (int q = 0; q < WPL; ++q) {
         const int w = q * 32 + lane;
-        mw[q] = w < w_d ? ld_row<GR>(R + (size_t)i * w_d + w) : 0u;
+        mw[q] = w < w_d ? ld_row<GR>(R + (size_t)i * S + w) : 0u;
       }
-      cnt += DistCount<K - 3, WPL, STATS, GR>::run(mw, R, w_d, deg, elems);
+      cnt += DistCount<K - 3, WPL, STATS, GR>::run(mw, R, w_d, deg, elems, S);
     }
   }
   __syncthreads();

@@ -133,11 +133,12 @@ __global__ void __launch_bounds__(256) k_clique_warp(CliqueArgs a) {
 // GR: the bitmap rows live in global scratch (a.rows, dmax * W words per CTA, L2-resident)
 // and the shared memory holds only the root's list and row offsets.
 template <int K, bool STATS, bool ETRI = false, bool PAIRS = false, int ROWW = kCtaRowWords,
-          int WPL = 1, bool GR = false, bool TT = false>
+          int WPL = 1, bool GR = false, bool TT = false, bool BAL = false>
 __global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int W) {
   extern __shared__ __align__(16) unsigned char smem[];
   const MidSmem sm = MidSmem::carve(smem, dmax, W,
-                                    GR ? a.rows + (size_t)blockIdx.x * dmax * W : nullptr);
+                                    GR ? a.rows + (size_t)blockIdx.x * dmax * W : nullptr,
+                                    BAL ? ROWW : 0);
   __shared__ unsigned long long s_idx;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -148,8 +149,9 @@ __global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int 
     const int64_t idx = (int64_t)s_idx + a.begin;
     __syncthreads();
     if (idx >= a.end) break;
-    cnt += cta_root<K, STATS, ETRI, PAIRS, ROWW, WPL, GR, TT>(a.rowptr, a.col, a.roots[idx], sm,
-                                                              a.tri, elems, a.srow);
+    cnt += cta_root<K, STATS, ETRI, PAIRS, ROWW, WPL, GR, TT, BAL>(a.rowptr, a.col,
+                                                                   a.roots[idx], sm, a.tri,
+                                                                   elems, a.srow);
   }
   for (int o = 16; o > 0; o >>= 1) {
     cnt += __shfl_xor_sync(kFull, cnt, o);
@@ -276,6 +278,10 @@ constexpr int kWideBandRowWords() { return K == 4 || K == 5 ? 32 : 0; }
 
 // One CTA-root band: bitmap layout for out-degree <= dmax, masks of up to ROWW words counted
 // from registers, wider ones with WPL words per lane; GR puts the rows in global scratch.
+// A plain 5-clique count with rows in shared memory counts with the balanced form.
+template <int K, bool STATS, bool ETRI, int ROWW, bool GR>
+constexpr bool kBandBalanced() { return K == 5 && !STATS && !ETRI && ROWW > 0 && !GR; }
+
 template <int K, bool STATS, bool ETRI, bool PAIRS, int ROWW, int WPL = 1, bool GR = false,
           bool TT = false>
 void launch_mid_band(CliqueArgs a, const TierRange& r, int cursor, int dmax, int sms,
@@ -284,8 +290,10 @@ void launch_mid_band(CliqueArgs a, const TierRange& r, int cursor, int dmax, int
   a.end = r.e;
   a.cursor = cursor;
   const int W = (dmax + 31) / 32;
-  const size_t sm = GR ? MidLayout{dmax, W}.bytes_no_rows() : MidLayout{dmax, W}.bytes();
-  auto kern = k_clique_mid<K, STATS, ETRI, PAIRS, ROWW, WPL, GR, TT>;
+  constexpr bool BAL = kBandBalanced<K, STATS, ETRI, ROWW, GR>();
+  const MidLayout lay{dmax, W, BAL ? ROWW : 0};
+  const size_t sm = GR ? lay.bytes_no_rows() : lay.bytes();
+  auto kern = k_clique_mid<K, STATS, ETRI, PAIRS, ROWW, WPL, GR, TT, BAL>;
   raise_smem_limit((const void*)kern, sm);  // a failure shows up as the launch error
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, sm);
