@@ -10,8 +10,15 @@ set-op operand elements of the canonical edge-rooted plan (every level-1 arc int
 N+(u) & N+(v) adds d+(u)+d+(v), every deeper "W & N+(v)" adds |W|+d+(v)), counted exactly
 by the library's accounting pass and cross-checked against the oracle in the tests.
 Between timed steps L2 is flushed by writing a 512 MiB buffer (the graph is ~100 MB, below
-the 126 MB L2).  Multi-GPU (torchrun): every rank holds a replica and counts the full
-workload (weak scaling, replicas); the counts are summed with one NCCL all-reduce.
+the 126 MB L2).  Multi-GPU (torchrun): every rank holds the whole graph and counts its shard
+of each count (jgpm_count_shard: the roots of every out-degree tier with index = rank mod
+world), so the total work is fixed (strong scaling); the partial counts are summed with one
+NCCL all-reduce, and times are the maximum over ranks.
+
+The kernels are bound by instruction issue, not by memory (the DAG stays in L2): `roofline`
+reports the dominant count's issue-slot use (warp instructions per second, from the ncu
+counters committed in profiles/counters.json, over 4 issue slots x SMs x the sampled SM
+clock), with its DRAM and L2 traffic beside it.
 
 The reference arm (--impl reference) times the reference's own host code (its AVX2
 set-intersection and graph loader, compiled from its sources into oracle/_ref/) driving the
@@ -111,6 +118,37 @@ def dist_env():
 
 
 # ----------------------------------------------------------------------------- our arm
+def counters():
+    """Per-count ncu counters of the tier kernels (profiles/counters.json): warp instructions,
+    DRAM and L2 bytes of one 4-clique and one 5-clique count of this workload."""
+    p = os.path.join(ROOT, "profiles", "counters.json")
+    return json.load(open(p)) if os.path.exists(p) else {}
+
+
+def roofline_of(name, ms, elems, ctr, sm_mhz, sms, hbm, hbm_kind):
+    """Issue-slot roofline of one count: the tier kernels run from L2 and are bound by
+    instruction issue.  achieved = warp instructions (ncu) / the count's event-timed
+    duration; peak = 4 issue slots x SMs x the median SM clock sampled during the run."""
+    c = ctr.get(name)
+    t = ms / 1e3
+    out = {"bound": "issue", "kernel": f"{name} count (bitmap clique tiers)", "unit": "warp-inst/s",
+           "peak": 4.0 * sms * sm_mhz * 1e6,
+           "peak_kind": f"4 issue slots x {sms} SMs x {sm_mhz:.0f} MHz (median sampled SM clock)",
+           "algorithmic_gbs": 4.0 * elems / t / 1e9,
+           "algorithmic_note": "canonical plan's set-op operand bytes per second: a work rate, "
+                               "not memory traffic (the bitmap kernels read far fewer bytes)"}
+    if c:
+        out.update({"achieved": c["warp_inst"] / t, "frac": c["warp_inst"] / t / out["peak"],
+                    "warp_inst_per_launch": c["warp_inst"], "traffic": c["dram_bytes"],
+                    "dram_gbs": c["dram_bytes"] / t / 1e9,
+                    "dram_frac": c["dram_bytes"] / t / 1e9 / hbm, "dram_peak_gbs": hbm,
+                    "dram_peak_kind": hbm_kind, "l2_bytes": c["l2_bytes"],
+                    "l2_gbs": c["l2_bytes"] / t / 1e9, "counters": "profiles/counters.json"})
+    else:
+        out.update({"achieved": None, "frac": None, "traffic": None})
+    return out
+
+
 def run_jgpm(args):
     import ctypes
 
@@ -118,6 +156,7 @@ def run_jgpm(args):
     import torch
 
     import jupiter_b200 as J
+    from jupiter_b200 import shards
 
     rank, local, world = dist_env()
     torch.cuda.set_device(local)
@@ -127,6 +166,7 @@ def run_jgpm(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
 
     g = J.Graph.rmat(N_VERT, EDGE_FACTOR, 0.57, 0.19, 0.19, 1, use_dag=True)
     info = g.info()
@@ -140,21 +180,35 @@ def run_jgpm(args):
     elems_step = elems4 + elems5
     matches_step = c4 + c5
 
+    def count(pattern):
+        if world > 1:
+            return g.count_shard(pattern, rank, world, details=True)
+        return g.count(pattern, details=True)
+
+    if world > 1:  # the shards add up to the whole count on every rank
+        parts = [count("4-clique")[0], count("5-clique")[0]]
+        if shards.reduce_counts(parts, dev) != [c4, c5]:
+            raise RuntimeError("sharded counts do not add up to the whole counts")
+    want = None
+
     def step(events):
+        nonlocal want
         with torch.cuda.stream(stream):
             flush.fill_(1)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e2 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-        a, sa = g.count("4-clique", details=True)
+        a, sa = count("4-clique")
         with torch.cuda.stream(stream):
             e1.record(stream)
-        b, sb = g.count("5-clique", details=True)
+        b, sb = count("5-clique")
         with torch.cuda.stream(stream):
             e2.record(stream)
-        if a != c4 or b != c5:
-            raise RuntimeError(f"count changed between runs: {a} {b} vs {c4} {c5}")
+        if want is None:
+            want = (a, b)
+        if (a, b) != want:
+            raise RuntimeError(f"count changed between runs: {a} {b} vs {want}")
         events.append((e0, e1, e2, sa["launches"] + sb["launches"]))
 
     for _ in range(args.warmup):
@@ -173,18 +227,18 @@ def run_jgpm(args):
     torch.cuda.synchronize()
     t4 = [e0.elapsed_time(e1) for e0, e1, e2, _ in events]
     t5 = [e1.elapsed_time(e2) for e0, e1, e2, _ in events]
-    step_ms = [a + b for a, b in zip(t4, t5)]
-    total_ms = sum(step_ms)
+    total_ms = sum(a + b for a, b in zip(t4, t5))
     launches = sum(x[3] for x in events)
+    k4_ms, k5_ms = sum(t4) / len(t4), sum(t5) / len(t5)
     if world > 1:
-        from jupiter_b200 import replicas
-        total_ms = replicas.max_over_ranks(total_ms, dev)
-        replicas.check_replicas([c4, c5], dev)  # the one exchange: the summed counts
+        total_ms = shards.max_over_ranks(total_ms, dev)
+        k4_ms = shards.max_over_ranks(k4_ms, dev)
+        k5_ms = shards.max_over_ranks(k5_ms, dev)
     ms_per_step = total_ms / args.steps
-    value = world * elems_step / (ms_per_step / 1e3)
+    value = elems_step / (ms_per_step / 1e3)
 
-    # e2e: through the public API with host buffers (pinned), H2D + orientation + both
-    # counts + the result read-back inside the timed region
+    # e2e: through the public API with host buffers (pinned): upload of the CSR, orientation,
+    # both counts (this rank's shards), the counts read back (and summed over the ranks)
     rowptr, col = g.csr()
     h_rowptr = torch.from_numpy(rowptr).pin_memory()
     h_col = torch.from_numpy(col).pin_memory()
@@ -200,60 +254,63 @@ def run_jgpm(args):
         if rc:
             raise RuntimeError(J.lib().jgpm_last_error().decode())
         gg = J.Graph(h.value)
-        a = gg.count("4-clique")
-        b = gg.count("5-clique")
+        if world > 1:
+            parts = [gg.count_shard("4-clique", rank, world),
+                     gg.count_shard("5-clique", rank, world)]
+            a, b = shards.reduce_counts(parts, dev)
+        else:
+            a, b = gg.count("4-clique"), gg.count("5-clique")
         gg.close()
         if a != c4 or b != c5:
             raise RuntimeError("e2e count mismatch")
 
     # each e2e step is timed on its own (host clock around a synchronous call) and the median
-    # is reported: the host-side part (allocation, upload, orientation) varies from step to step
-    e2e_steps = max(3, min(args.steps, 7))
+    # over all timed steps is reported: the host-side part varies from step to step
     e2e_step()
     torch.cuda.synchronize()
     e2e_times = []
-    for _ in range(e2e_steps):
+    for _ in range(args.steps):
+        if world > 1:
+            dist.barrier()
         t0 = time.perf_counter()
         e2e_step()
         torch.cuda.synchronize()
         e2e_times.append((time.perf_counter() - t0) * 1e3)
     e2e_ms = statistics.median(e2e_times)
     if world > 1:
-        e2e_ms = replicas.max_over_ranks(e2e_ms, dev)
+        e2e_ms = shards.max_over_ranks(e2e_ms, dev)
     h2d = rowptr.nbytes + col.nbytes
     d2h = 2 * 8
 
-    peak, peak_kind = peaks()
-    k4_ms = sum(t4) / len(t4)
-    achieved = 4.0 * elems4 / (k4_ms / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("4-clique_bytes_per_launch")
+    hbm, hbm_kind = peaks()
+    ck = clk.summary()
+    sm_mhz = ck["sm_mhz"] or 1965.0
+    ctr = counters()
+    roof = roofline_of("5-clique", k5_ms, elems5, ctr, sm_mhz, sms, hbm, hbm_kind)
+    roof["other"] = {"4-clique": roofline_of("4-clique", k4_ms, elems4, ctr, sm_mhz, sms, hbm,
+                                             hbm_kind)}
+    roof["kernel_share_of_step"] = k5_ms / ms_per_step
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded R-MAT stands in for the absent citation dataset)",
-        "config": dict(WORKLOAD, parallelism=f"replicas{world}" if world > 1 else "single",
+        "config": dict(WORKLOAD, parallelism=f"root shards x{world}" if world > 1 else "single",
                        num_vertices=info["num_vertices"], num_arcs=info["num_arcs"],
                        num_dag_arcs=info["num_dag_arcs"],
                        max_out_degree=info["max_out_degree"]),
-        "matches_per_s": world * matches_step / (ms_per_step / 1e3),
+        "matches_per_s": matches_step / (ms_per_step / 1e3),
         "counts": {"4-clique": c4, "5-clique": c5},
         "setop_elements": {"4-clique": elems4, "5-clique": elems5},
-        "ms": {"4-clique": k4_ms, "5-clique": sum(t5) / len(t5)},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "4-clique count (bitmap clique tiers)", "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": 4 * elems4},
-        "e2e": {"value": world * elems_step / (e2e_ms / 1e3), "unit": UNIT,
+        "ms": {"4-clique": k4_ms, "5-clique": k5_ms},
+        "roofline": roof,
+        "e2e": {"value": elems_step / (e2e_ms / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                "steps": e2e_steps, "ms_min": min(e2e_times), "ms_max": max(e2e_times),
+                "steps": len(e2e_times), "ms_min": min(e2e_times), "ms_max": max(e2e_times),
                 "stat": "median of per-step times"},
         "gpu_launches": launches,
-        "clocks": clk.summary(),
+        "clocks": ck,
     }
     g.close()
     if rank == 0 and not args.no_cpu_baseline:

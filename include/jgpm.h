@@ -165,6 +165,18 @@ int jgpm_count_ex(jgpm_graph* g, const char* pattern, int induced, int chunk_siz
 int jgpm_count_roots(jgpm_graph* g, const char* pattern, int induced, int64_t begin,
                      int64_t end, int64_t stride, uint64_t* out, jgpm_stats* st);
 
+/* The part of jgpm_count's result that shard `shard` of `nshards` owns, for splitting one
+ * count over several GPUs (each holding the whole graph): the shards' results add up to the
+ * full count, so one sum over the shards -- an all-reduce of one uint64 per count -- gives
+ * it.  k-cliques ("triangle", "4-clique" .. "k-clique:<k>") shard the roots of every
+ * out-degree tier of the bitmap kernels: shard s takes tier indices s, s + nshards, ..., so
+ * every shard gets the same mix of heavy and light roots.  Every other pattern runs its
+ * nested-loop plan (as jgpm_count_roots) over the root arcs shard, shard + nshards, ....
+ * Replaces the reference's split of the root edges over ranks (src/jupiter_gpm.cu:91-150)
+ * and its sum of the ranks' counts (:880-904). */
+int jgpm_count_shard(jgpm_graph* g, const char* pattern, int induced, int32_t shard,
+                     int32_t nshards, uint64_t* out, jgpm_stats* st);
+
 /* Allocation-free count.  No counterpart in the reference: it exists for callers that may
  * not allocate device memory while they count (a host whose own allocator holds the device,
  * or a latency-critical path that must not call cudaMalloc/cudaFree).  It calls no

@@ -142,6 +142,8 @@ def lib():
                                 _PU64, ctypes.POINTER(_Stats)]
     L.jgpm_count_roots.argtypes = [G, ctypes.c_char_p, ctypes.c_int, ctypes.c_int64,
                                    ctypes.c_int64, ctypes.c_int64, _PU64, ctypes.POINTER(_Stats)]
+    L.jgpm_count_shard.argtypes = [G, ctypes.c_char_p, ctypes.c_int, ctypes.c_int32,
+                                   ctypes.c_int32, _PU64, ctypes.POINTER(_Stats)]
     L.jgpm_census4.argtypes = [G, _PU64, ctypes.POINTER(_Stats)]
     L.jgpm_setop.argtypes = [ctypes.c_int, _P32, ctypes.c_int32, _P32, ctypes.c_int32,
                              ctypes.c_int32, ctypes.c_int32, _P32, _P32]
@@ -296,6 +298,17 @@ class Graph:
                                       ctypes.byref(st)))
         if details:
             return out.value, {"kernel_ms": st.kernel_ms, "launches": st.launches}
+        return out.value
+
+    def count_shard(self, pattern, shard, nshards, induced=False, details=False):
+        """Shard `shard` of `nshards` of the count of `pattern`; the shards add up to it."""
+        out = ctypes.c_uint64()
+        st = _Stats()
+        _check(lib().jgpm_count_shard(self._h, pattern.encode(), int(bool(induced)), int(shard),
+                                      int(nshards), ctypes.byref(out), ctypes.byref(st)))
+        if details:
+            return out.value, {"kernel_ms": st.kernel_ms, "launches": st.launches,
+                               "method": METHODS.get(st.method, st.method)}
         return out.value
 
     def census4(self):

@@ -27,6 +27,7 @@ int edges_build(jgpm_graph* g, const int32_t* src, const int32_t* dst, int64_t n
 int launch_clique(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64_t root_end,
                   cudaStream_t s);
 int launch_level1_elements(jgpm_graph* g, cudaStream_t s);
+int launch_clique_shard(jgpm_graph* g, int k, int shard, int nshards, cudaStream_t s);
 }  // namespace jgpm
 
 using namespace jgpm;
@@ -438,6 +439,72 @@ int jgpm_count_roots(jgpm_graph* g, const char* pattern, int induced, int64_t be
     st->kernel_ms = ms;
     st->rounds = 1;
     st->method = JGPM_METHOD_PLAN;
+    st->launches = g->launches;
+  }
+  return JGPM_OK;
+}
+
+int jgpm_count_shard(jgpm_graph* g, const char* pattern, int induced, int32_t shard,
+                     int32_t nshards, uint64_t* out, jgpm_stats* st) {
+  if (!g || !pattern || !out) {
+    jgpm_set_error_("jgpm_count_shard: null argument");
+    return JGPM_EINVAL;
+  }
+  if (nshards < 1 || shard < 0 || shard >= nshards) {
+    jgpm_set_error_("jgpm_count_shard: need 0 <= shard < nshards");
+    return JGPM_EINVAL;
+  }
+  ScopedDevice sd(g->device);
+  const std::string p(pattern);
+  const int k = clique_k_of(p);
+  if (k < 0) {
+    jgpm_set_error_("jgpm_count_shard: k-clique needs 3 <= k <= 8");
+    return JGPM_EPATTERN;
+  }
+  g->launches = 0;
+  uint64_t count = 0;
+  double ms = 0.0;
+  int method = 0;
+  int rc;
+  if (k > 0) {
+    if ((rc = ensure_dag(g))) return rc;
+    if ((rc = ensure_tiers(g, k - 1))) return rc;
+    if ((rc = ensure_control(g))) return rc;
+    cudaStream_t s = g->stream;
+    cudaEvent_t e0, e1;
+    JGPM_CUDA_TRY(cudaEventCreate(&e0));
+    JGPM_CUDA_TRY(cudaEventCreate(&e1));
+    if ((rc = reset_control(g, s))) return rc;
+    JGPM_CUDA_TRY(cudaEventRecord(e0, s));
+    if ((rc = launch_clique_shard(g, k, shard, nshards, s))) return rc;
+    JGPM_CUDA_TRY(cudaEventRecord(e1, s));
+    if ((rc = read_control(g, s))) return rc;
+    float fms = 0.f;
+    cudaEventElapsedTime(&fms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    count = g->h_ctl->count[0];
+    ms = fms;
+    method = JGPM_METHOD_BITMAP_CLIQUE;
+  } else {
+    const int id = literal_plan_id(p, induced);
+    if (id < 0) {
+      jgpm_set_error_("jgpm_count_shard: no nested-loop plan for '" + p + "'" +
+                      (induced ? " (vertex-induced)" : ""));
+      return JGPM_EPATTERN;
+    }
+    const int64_t m = plan_root_arcs(g, id);
+    if (m < 0) return JGPM_ECUDA;
+    if ((rc = count_roots_impl(g, id, shard, m, nshards, &count, &ms))) return rc;
+    method = JGPM_METHOD_PLAN;
+  }
+  *out = count;
+  if (st) {
+    memset(st, 0, sizeof(*st));
+    st->count = count;
+    st->kernel_ms = ms;
+    st->rounds = 1;
+    st->method = method;
     st->launches = g->launches;
   }
   return JGPM_OK;

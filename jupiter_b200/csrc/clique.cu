@@ -59,7 +59,7 @@ __global__ void k_level1_elements(const eid_t* rowptr, const vid_t* col, vid_t n
 // Root ranges of a k-clique count over tier indices [root_begin, root_end): roots with
 // d >= k-1 only, split by out-degree into the group widths allowed by min_group.
 static TierPlan make_plan(const RootTiers& t, int k, int64_t root_begin, int64_t root_end,
-                          int min_group, int split) {
+                          int min_group, int split, int shard, int nshards) {
   const int64_t stop = std::min(root_end, t.deg_begin[k - 2 >= 0 ? k - 2 : 0]);
   auto cut = [&](int64_t b, int64_t e) {
     TierRange r{std::max(b, root_begin), std::min(e, stop)};
@@ -86,6 +86,17 @@ static TierPlan make_plan(const RootTiers& t, int k, int64_t root_begin, int64_t
   p.g16 = cut(std::max(t.mid_end, b16), std::max(b16, b8));
   p.g8 = cut(std::max(b16, b8), std::max(b8, b4));
   p.g4 = cut(std::max(b8, b4), t.small_end);
+  if (nshards > 1) {
+    // shard s of n takes tier indices b + s, b + s + n, ... of every range, so each shard gets
+    // an equal share of every out-degree band
+    TierRange* all[] = {&p.large, &p.wide, &p.mid[0], &p.mid[1], &p.mid[2], &p.warp,
+                        &p.g32, &p.g16, &p.g8, &p.g4};
+    for (TierRange* r : all) {
+      const int64_t b = r->b + shard;
+      const int64_t cnt = b < r->e ? (r->e - b + nshards - 1) / nshards : 0;
+      *r = TierRange{b, b + cnt, nshards};
+    }
+  }
   return p;
 }
 
@@ -95,7 +106,7 @@ static TierPlan make_plan(const RootTiers& t, int k, int64_t root_begin, int64_t
 // The caller zeroes the work cursors before each call.
 int launch_clique_ex(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64_t root_end,
                      cudaStream_t s, uint32_t* tri, int min_group, bool pairs = false,
-                     bool tt = false) {
+                     bool tt = false, int shard = 0, int nshards = 1) {
   if (k < 3 || k > 8) {
     jgpm_set_error_("k-clique: k must be in [3, 8]");
     return JGPM_EPATTERN;
@@ -104,8 +115,9 @@ int launch_clique_ex(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64
   const RootTiers& t = g->tiers;
   // every triangle needs its root (out-degree >= 2) in the edge-triangle modes
   const TierPlan p = make_plan(t, (stats || tri) ? 3 : k, root_begin, root_end, min_group,
-                               g->tune_split);
+                               g->tune_split, shard, nshards);
   CliqueArgs a{};
+  a.step = 1;
   a.rowptr = g->d_dag_rowptr;
   a.col = g->d_dag_col;
   a.roots = t.d_roots;
@@ -154,6 +166,12 @@ int launch_clique_ex(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64
 int launch_clique(jgpm_graph* g, int k, bool stats, int64_t root_begin, int64_t root_end,
                   cudaStream_t s) {
   return launch_clique_ex(g, k, stats, root_begin, root_end, s, nullptr, g->tune_min_group);
+}
+
+// One shard of a k-clique count: the roots of every tier with index = shard (mod nshards).
+int launch_clique_shard(jgpm_graph* g, int k, int shard, int nshards, cudaStream_t s) {
+  return launch_clique_ex(g, k, false, 0, g->tiers.deg_begin[k - 2], s, nullptr,
+                          g->tune_min_group, false, false, shard, nshards);
 }
 
 // Triangles per DAG arc into d_tri (zeroed by the caller); the triangle total also

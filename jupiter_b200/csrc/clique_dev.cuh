@@ -504,6 +504,23 @@ __host__ __device__ __forceinline__ size_t bal_bytes(int rw) {
   return rw > 0 ? (size_t)8 * ((size_t)rw * 32 * 4 + (size_t)kBalCap * 2) : 0;
 }
 
+// Level-2 bitmaps of the 5-clique count (rows of up to 16 words): per warp, the positions of
+// the members of one row R_i (kL2Max of them) and their induced adjacency, kL2Stride words
+// per member (odd, so that 32 members' words fall into 32 banks).
+constexpr int kL2Max = 128;
+constexpr int kL2Words = kL2Max / 32;
+constexpr int kL2Stride = kL2Words + 1;
+__host__ __device__ __forceinline__ size_t l2_bytes() {
+  return (size_t)8 * ((size_t)kL2Max * kL2Stride * 4 + (size_t)kL2Max * 2);
+}
+// Buffers of the balanced 5-clique count for masks of rw words: a row counter, then the
+// level-2 buffers (rw <= 16) or the item buffers (rw = 32), over the same memory.
+__host__ __device__ __forceinline__ size_t k5_bytes(int rw) {
+  if (rw <= 0) return 0;
+  const size_t b = rw <= 16 ? l2_bytes() : bal_bytes(rw);
+  return 16 + b + 16;  // counter, buffers, alignment slack
+}
+
 // Shared layout for one mid-tier root (dynamic shared memory):
 //   L[dmax] ids | off[dmax+1] exclusive row offsets | rs[dmax] row starts (int64) |
 //   deg[dmax] | ln[dmax] row lengths | R[dmax * row_stride(W)] rows | 8 warp sums |
@@ -516,7 +533,7 @@ struct MidLayout {
   }
   __host__ __device__ size_t bytes_no_rows() const {
     return (size_t)dmax * 4 + (size_t)(dmax + 1) * 4 + (size_t)dmax * 8 + (size_t)dmax * 8 +
-           64 + 64 + bal_bytes(bal_rw) + (bal_rw > 0 ? 16 : 0);
+           64 + 64 + k5_bytes(bal_rw);
   }
 };
 
@@ -528,8 +545,11 @@ struct MidSmem {
   int* ln;  // row lengths after the range cut
   uint32_t* R;
   int* wsum;
-  uint32_t* bal_m;     // balanced count: 8 warps x RW x 32 mask words
-  uint16_t* bal_list;  // balanced count: 8 warps x kBalCap items
+  int* k5_next;        // balanced 5-clique count: next row to take (level-2 form)
+  uint32_t* bal_m;     // item form: 8 warps x RW x 32 mask words
+  uint16_t* bal_list;  // item form: 8 warps x kBalCap items
+  uint32_t* l2_a;      // level-2 form: 8 warps x kL2Max x kL2Stride adjacency words
+  uint16_t* l2_p;      // level-2 form: 8 warps x kL2Max member positions
   // rows = nullptr: the rows follow in shared memory (MidLayout); otherwise they live at
   // rows (dmax * W words of global scratch for this CTA) and shared memory holds the rest
   // (MidLayout::bytes_no_rows).
@@ -550,9 +570,12 @@ struct MidSmem {
       m.R = after;
       m.wsum = reinterpret_cast<int*>(m.R + (size_t)dmax * row_stride(W, false));
     }
-    m.bal_m = reinterpret_cast<uint32_t*>(
+    m.k5_next = reinterpret_cast<int*>(
         (reinterpret_cast<uintptr_t>(m.wsum + 8) + 15) & ~uintptr_t(15));
+    m.bal_m = reinterpret_cast<uint32_t*>(m.k5_next + 4);
     m.bal_list = reinterpret_cast<uint16_t*>(m.bal_m + (size_t)8 * bal_rw * 32);
+    m.l2_a = m.bal_m;
+    m.l2_p = reinterpret_cast<uint16_t*>(m.l2_a + (size_t)8 * kL2Max * kL2Stride);
     return m;
   }
 };
@@ -698,6 +721,117 @@ __device__ __forceinline__ acc_t bal_count5(const int* off, int d, int topO,
   return cnt;
 }
 
+// 5-cliques through row i of a root: the triangles of the sub-DAG that the rows induce on the
+// c members of R_i (c <= 32 P), counted by one warp.  The members' positions go to Pw; the
+// induced adjacency A (member x -> member y iff position p_y is in row p_x) is built one
+// member at a time with a ballot per 32 members, into Aw (kL2Stride words per member); then
+// lane x sums popc(A_x & A_y) over the y in A_x.  Every mask is P words instead of the
+// row's w_d, and no lane waits for another.
+template <int P>
+__device__ __forceinline__ int l2_row(const uint32_t* Ri, int w_d, int c, const uint32_t* R,
+                                      int S, uint32_t* Aw, uint16_t* Pw) {
+  const int lane = threadIdx.x & 31;
+  {  // member positions: word q of R_i on lane q, inclusive prefix of the word popcounts
+    const uint32_t wq = lane < w_d ? Ri[lane] : 0u;
+    int incl = __popc(wq);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int excl = incl - __popc(wq);
+#pragma unroll
+    for (int w = 0; w < P; ++w) {
+      const int y = lane + 32 * w;
+      int q = 0;  // the word holding member y: the number of words ending at or before y
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int v = __shfl_sync(kFull, incl, q + step - 1);
+        if (v <= y) q += step;
+      }
+      const uint32_t word = __shfl_sync(kFull, wq, q & 31);
+      const int ex = __shfl_sync(kFull, excl, q & 31);
+      if (y < c) Pw[y] = (uint16_t)(q * 32 + (int)__fns(word, 0, y - ex + 1));
+    }
+  }
+  __syncwarp();
+  int pw[P], pb[P];  // word and bit of member y = lane + 32 w
+#pragma unroll
+  for (int w = 0; w < P; ++w) {
+    const int y = lane + 32 * w;
+    const int p = y < c ? (int)Pw[y] : 0;
+    pw[w] = p >> 5;
+    pb[w] = p & 31;
+  }
+  for (int x = 0; x < c; ++x) {
+    const uint32_t* Rx = R + (size_t)Pw[x] * S;
+#pragma unroll
+    for (int w = 0; w < P; ++w) {
+      const bool b = lane + 32 * w < c && ((Rx[pw[w]] >> pb[w]) & 1u);
+      const uint32_t m = __ballot_sync(kFull, b);
+      if (lane == w) Aw[x * kL2Stride + w] = m;
+    }
+  }
+  __syncwarp();
+  int s = 0;
+#pragma unroll
+  for (int pass = 0; pass < P; ++pass) {
+    const int x = lane + 32 * pass;
+    uint32_t ax[P];
+#pragma unroll
+    for (int w = 0; w < P; ++w) ax[w] = x < c ? Aw[x * kL2Stride + w] : 0u;
+#pragma unroll
+    for (int wy = 0; wy < P; ++wy) {
+      const int ylim = min(32, c - 32 * wy);
+      for (int yb = 0; yb < ylim; ++yb) {
+        const uint32_t* Ay = Aw + (32 * wy + yb) * kL2Stride;
+        int t = 0;
+#pragma unroll
+        for (int w = 0; w < P; ++w) t += __popc(ax[w] & Ay[w]);
+        s += ((ax[wy] >> yb) & 1u) ? t : 0;
+      }
+    }
+  }
+  __syncwarp();
+  return s;
+}
+
+// 5-cliques of one root through the level-2 bitmaps of each row, rows taken by the CTA's warps
+// from a shared counter; rows of more than kL2Max members are counted pair by pair.
+template <int RW>
+__device__ __forceinline__ acc_t l2_count5(const uint32_t* R, int d, int w_d, int S,
+                                           int* next, uint32_t* Aw, uint16_t* Pw,
+                                           const int* deg, acc_t& elems) {
+  const int lane = threadIdx.x & 31;
+  acc_t cnt = 0;
+  for (;;) {
+    int i = 0;
+    if (lane == 0) i = atomicAdd(next, 1);
+    i = __shfl_sync(kFull, i, 0);
+    if (i >= d) break;
+    const uint32_t* Ri = R + (size_t)i * S;
+    int c = 0;
+#pragma unroll
+    for (int q = 0; q < RW; ++q) c += q < w_d ? __popc(Ri[q]) : 0;
+    if (c < 3) continue;
+    if (c <= 32) cnt += (acc_t)l2_row<1>(Ri, w_d, c, R, S, Aw, Pw);
+    else if (c <= 64) cnt += (acc_t)l2_row<2>(Ri, w_d, c, R, S, Aw, Pw);
+    else if (c <= 96) cnt += (acc_t)l2_row<3>(Ri, w_d, c, R, S, Aw, Pw);
+    else if (c <= kL2Max) cnt += (acc_t)l2_row<4>(Ri, w_d, c, R, S, Aw, Pw);
+    else {  // a dense row: its pairs (i, j) one per lane
+      for (int jj = lane; jj < c; jj += 32) {
+        const int j = select_bit(Ri, w_d, jj);
+        const uint32_t* Rj = R + (size_t)j * S;
+        uint32_t m2[RW];
+#pragma unroll
+        for (int q = 0; q < RW; ++q) m2[q] = q < w_d ? (Ri[q] & Rj[q]) : 0u;
+        cnt += RowCount<1, RW, false>::run(m2, R, w_d, deg, elems, S);
+      }
+    }
+  }
+  return cnt;
+}
+
 // One root of out-degree 32 < d <= dmax processed by the whole CTA (blockDim = 256).
 // Every thread calls it; returns this thread's partial count.  Rows of up to ROWW words are
 // counted row-parallel from registers, wider ones (or all, with ROWW = 0) warp-cooperatively
@@ -821,7 +955,13 @@ __device__ __forceinline__ acc_t cta_root(const eid_t* __restrict__ rowptr,
   acc_t cnt = 0;
   static_assert(!GR || ROWW == 0, "rows in global memory are counted warp-cooperatively");
   constexpr int RW = ROWW > 0 ? ROWW : 1;
-  if (ROWW > 0 && w_d <= ROWW && K >= 5 && !ETRI) {
+  if (BAL && RW <= 16 && w_d <= ROWW) {
+    // 5-cliques through level-2 bitmaps, one row per warp (rows from a shared counter)
+    if (tid == 0) *sm.k5_next = 0;
+    __syncthreads();
+    cnt += l2_count5<RW>(R, d, w_d, S, sm.k5_next, sm.l2_a + (size_t)warp * kL2Max * kL2Stride,
+                         sm.l2_p + (size_t)warp * kL2Max, deg, elems);
+  } else if (ROWW > 0 && w_d <= ROWW && K >= 5 && !ETRI) {
     // k >= 5: the first two levels flattened over the threads as (row i, bit j of R_i)
     // pairs, so one dense row does not hold up the CTA.  off[i] = pairs before row i.
     for (int i = tid; i < d; i += nthreads) {

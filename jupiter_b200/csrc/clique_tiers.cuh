@@ -16,7 +16,8 @@ struct CliqueArgs {
   const eid_t* rowptr;  // DAG row pointers
   const vid_t* col;     // DAG neighbour lists
   const vid_t* roots;
-  int64_t begin, end;   // root range of this launch
+  int64_t begin, end;   // root range of this launch: roots[begin + (i - begin) * step],
+  int64_t step;         // begin <= i < end (step > 1: one shard's roots of a tier)
   DevControl* ctl;
   int32_t* scratch;     // large tier: per-warp lists
   int64_t scratch_per_warp;
@@ -32,10 +33,17 @@ struct CliqueArgs {
 
 constexpr int kMaxLevels = 6;  // list tier: candidate lists per warp
 
+// Tier indices b, b + step, ..., (e - b) of them.
 struct TierRange {
   int64_t b, e;
+  int64_t step = 1;
   bool empty() const { return e <= b; }
 };
+
+// Root of launch index i (a.begin <= i < a.end).
+__device__ __forceinline__ vid_t root_at(const CliqueArgs& a, int64_t i) {
+  return a.roots[a.begin + (i - a.begin) * a.step];
+}
 
 // Launch plan of one count: the root ranges of each tier.  wide holds the CTA roots of
 // out-degree (1024, 4096] (rows in global scratch); mid[0..2] are the CTA-root bands of
@@ -89,7 +97,7 @@ __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
     const int64_t first = a.begin + (int64_t)c0;
     if (first >= a.end) break;
     const int64_t idx = first + gi;
-    const vid_t u = idx < a.end ? a.roots[idx] : -1;
+    const vid_t u = idx < a.end ? root_at(a, idx) : -1;
     cnt += group_root<G, K, STATS, ETRI, PAIRS, TT>(a.rowptr, a.col, u, R, DG, a.tri, elems,
                                                      a.srow);
   }
@@ -116,7 +124,7 @@ __global__ void __launch_bounds__(256) k_clique_warp(CliqueArgs a) {
     c0 = __shfl_sync(kFull, c0, 0);
     const int64_t idx = a.begin + (int64_t)c0;
     if (idx >= a.end) break;
-    cnt += warp_root<K, STATS, ETRI, PAIRS, TT>(a.rowptr, a.col, a.roots[idx], ws, a.tri, elems,
+    cnt += warp_root<K, STATS, ETRI, PAIRS, TT>(a.rowptr, a.col, root_at(a, idx), ws, a.tri, elems,
                                                  a.srow);
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -150,7 +158,7 @@ __global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int 
     __syncthreads();
     if (idx >= a.end) break;
     cnt += cta_root<K, STATS, ETRI, PAIRS, ROWW, WPL, GR, TT, BAL>(a.rowptr, a.col,
-                                                                   a.roots[idx], sm, a.tri,
+                                                                   root_at(a, idx), sm, a.tri,
                                                                    elems, a.srow);
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -207,7 +215,7 @@ __global__ void __launch_bounds__(256) k_clique_large(CliqueArgs a) {
     t = __shfl_sync(kFull, t, 0);
     const int64_t r = a.begin + (int64_t)(t / (unsigned long long)a.large_chunks);
     if (r >= a.end) break;
-    const vid_t u = a.roots[r];
+    const vid_t u = root_at(a, r);
     const eid_t bu = a.rowptr[u];
     const int du = (int)(a.rowptr[u + 1] - bu);
     const int i0 = (int)(t % (unsigned long long)a.large_chunks) * 32;
@@ -288,6 +296,7 @@ void launch_mid_band(CliqueArgs a, const TierRange& r, int cursor, int dmax, int
                      cudaStream_t s) {
   a.begin = r.b;
   a.end = r.e;
+  a.step = r.step;
   a.cursor = cursor;
   const int W = (dmax + 31) / 32;
   constexpr bool BAL = kBandBalanced<K, STATS, ETRI, ROWW, GR>();
@@ -313,6 +322,7 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
   if (!p.large.empty()) {
     a.begin = p.large.b;
     a.end = p.large.e;
+    a.step = p.large.step;
     a.cursor = 2;
     k_clique_large<K, STATS, ETRI, PAIRS, TT><<<sms * 2, 256, 0, s>>>(a);
     ++n;
@@ -346,6 +356,7 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
   if (!p.warp.empty()) {
     a.begin = p.warp.b;
     a.end = p.warp.e;
+    a.step = p.warp.step;
     a.cursor = 7;
     const size_t sm = 8 * sizeof(WarpSmem);
     raise_smem_limit((const void*)k_clique_warp<K, STATS, ETRI, PAIRS, TT>, sm);
@@ -362,6 +373,7 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     if (gr[q]->empty()) continue;
     a.begin = gr[q]->b;
     a.end = gr[q]->e;
+    a.step = gr[q]->step;
     a.cursor = 3 + q;
     switch (q) {
       case 0: k_clique_group<32, K, STATS, ETRI, PAIRS, TT><<<sms * 8, 256, 0, s>>>(a); break;

@@ -62,3 +62,50 @@ def test_root_samples_reject_bad_arguments(gpu, graph):
         with pytest.raises(gpu.JgpmError) as e:
             g.count_roots(*args)
         assert e.value.code == code, args
+
+
+SHARD_PATTERNS = [("triangle", 0), ("4-clique", 0), ("5-clique", 0), ("k-clique:6", 0),
+                  ("k-clique:8", 0), ("P1", 0), ("P2", 0), ("P5", 0), ("4-cycle", 1),
+                  ("tailed-triangle", 1)]
+
+
+@pytest.mark.parametrize("name,induced", SHARD_PATTERNS)
+def test_shards_add_up_to_the_count(graph, name, induced):
+    g = graph[0]
+    full = g.count(name, induced=bool(induced))
+    for n in (2, 3, 7):
+        parts = [g.count_shard(name, r, n, induced=bool(induced)) for r in range(n)]
+        assert sum(parts) == full, (name, n, parts, full)
+    assert g.count_shard(name, 0, 1, induced=bool(induced)) == full
+
+
+def test_shards_cover_every_tier(gpu):
+    """K_1101 puts roots in the edge-rooted list tier (out-degree > 1024 in the DAG of K_n is
+    reached by ids 0..75), the wide bitmap band and every other tier; the crown's hub and
+    B vertices (out-degree 5000) take the list tier's chunked tasks.  The shards add up."""
+    from math import comb
+    n = 1101
+    iu = np.triu_indices(n, 1)
+    with gpu.Graph.from_edges(iu[0].astype(np.int32), iu[1].astype(np.int32), n) as g:
+        for k, want in ((3, comb(n, 3)), (4, comb(n, 4))):
+            for ns in (2, 5):
+                assert sum(g.count_shard(f"k-clique:{k}", r, ns) for r in range(ns)) == want
+    na, nb, grp = 5000, 5001, 1250
+    a = np.arange(na, dtype=np.int64)
+    b = np.arange(na, na + nb, dtype=np.int64)
+    h = na + nb
+    gq = a.reshape(grp, 4)
+    t = np.triu_indices(4, 1)
+    s = np.concatenate([np.repeat(a, nb), np.full(na, h), gq[:, t[0]].ravel()]).astype(np.int32)
+    d = np.concatenate([np.tile(b, na), a, gq[:, t[1]].ravel()]).astype(np.int32)
+    with gpu.Graph.from_edges(s, d, h + 1) as g:
+        for ns in (2, 3):
+            assert sum(g.count_shard("5-clique", r, ns) for r in range(ns)) == grp * (1 + nb)
+
+
+def test_shard_arguments(gpu, graph):
+    g = graph[0]
+    for args in (("4-clique", 2, 2), ("4-clique", -1, 2), ("P1", 0, 0)):
+        with pytest.raises(gpu.JgpmError) as e:
+            g.count_shard(*args)
+        assert e.value.code == -1, args
