@@ -610,13 +610,14 @@ def run_count(args):
     spec = (int(f[0]), int(f[1]), float(f[2]), float(f[3]), float(f[4]), int(f[5]))
     with J.Graph.rmat(*spec) as g:
         for _ in range(args.warmup):
-            c = g.count(args.pattern)
+            c = g.count(args.pattern, induced=args.induced)
         ms = []
         for _ in range(args.steps):
-            c, st = g.count(args.pattern, details=True)
+            c, st = g.count(args.pattern, induced=args.induced, details=True)
             ms.append(st["kernel_ms"])
-        print(json.dumps({"workload": "count", "pattern": args.pattern, "rmat": list(spec),
-                          "count": c, "kernel_ms": ms, "graph": g.info()}), flush=True)
+        print(json.dumps({"workload": "count", "pattern": args.pattern, "induced": args.induced,
+                          "rmat": list(spec), "count": c, "kernel_ms": ms, "method": st["method"],
+                          "graph": g.info()}), flush=True)
 
 
 def main():
@@ -630,6 +631,7 @@ def main():
     ap.add_argument("--workload", default="clique",
                     choices=["clique", "batched", "served", "induced", "count"])
     ap.add_argument("--pattern", default="4-cycle")
+    ap.add_argument("--induced", action="store_true", help="count workload: vertex-induced")
     ap.add_argument("--rmat",
                     default="258730,32,0.471263918196369,0.13218402045090777,0.13218402045090777,2958",
                     help="count workload: n,ef,a,b,c,seed (default: the heaviest 4-cycle job "

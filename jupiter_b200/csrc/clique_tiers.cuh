@@ -140,9 +140,18 @@ __global__ void __launch_bounds__(256) k_clique_warp(CliqueArgs a) {
 // --------------------------------------------------- CTA tiers (32 < d <= kWideMaxDeg)
 // GR: the bitmap rows live in global scratch (a.rows, dmax * W words per CTA, L2-resident)
 // and the shared memory holds only the root's list and row offsets.
+// Register budget of the CTA bands (minimum resident CTAs per SM): the bitmap build and the
+// row-parallel counts run faster with room for their masks (4-clique band of out-degree
+// <= 256: 2.21 ms at the 32 registers the compiler picks by default, with a spill; 1.69 ms
+// at 56), the level-2 5-clique count at 64 registers, with four CTAs per SM (the item form
+// of the widest band needs more).
+template <bool BAL, int ROWW>
+constexpr int kMidMinBlocks() { return BAL && ROWW <= 16 ? 4 : 1; }
+
 template <int K, bool STATS, bool ETRI = false, bool PAIRS = false, int ROWW = kCtaRowWords,
           int WPL = 1, bool GR = false, bool TT = false, bool BAL = false>
-__global__ void __launch_bounds__(256) k_clique_mid(CliqueArgs a, int dmax, int W) {
+__global__ void __launch_bounds__(256, kMidMinBlocks<BAL, ROWW>()) k_clique_mid(CliqueArgs a, int dmax,
+                                                                        int W) {
   extern __shared__ __align__(16) unsigned char smem[];
   const MidSmem sm = MidSmem::carve(smem, dmax, W,
                                     GR ? a.rows + (size_t)blockIdx.x * dmax * W : nullptr,
