@@ -56,6 +56,50 @@ __device__ __forceinline__ void count_below2(const int* a, int n, int top, int x
   }
 }
 
+// Row elements staged per warp when a row is searched for the root's list.
+constexpr int kStage = 256;
+
+// Row i of a root's bitmap when the row (len elements from col + rsi, sorted) is longer than
+// the root's list L[0..d): the list is looked up in the row, as the reference does with the
+// shorter of two lists.  Used by the warp tier, whose lists (out-degree <= 128) are mostly
+// shorter than their rows; in the CTA bands the extra registers cost more than it saves.  A warp stages up to kStage row elements at a time in shared memory
+// (one coalesced copy), each lane binary-searches two list entries in them, and the ballot
+// of the hits of 32 entries is one word of the row (ORed into Ri, which starts at zero).
+// on_hit(j, e) runs for every hit in the edge-triangle modes (j = list index, e = the slot
+// of L[j] in the row).
+template <bool ETRI, typename F>
+__device__ __forceinline__ void flip_row(const vid_t* __restrict__ col, eid_t rsi, int len,
+                                         const vid_t* L, int d, int w_d, uint32_t* Ri,
+                                         vid_t* stage, F&& on_hit) {
+  const int lane = threadIdx.x & 31;
+  for (int c0 = 0; c0 < len; c0 += kStage) {
+    const int cl = min(kStage, len - c0);
+    __syncwarp();
+    for (int t = lane; t < cl; t += 32) stage[t] = __ldg(col + rsi + c0 + t);
+    __syncwarp();
+    const int top = top_pow2(cl);
+    for (int q0 = 0; q0 < w_d; q0 += 2) {
+      const int ja = 32 * q0 + lane, jb = ja + 32;
+      const vid_t xa = ja < d ? L[ja] : INT32_MAX;
+      const vid_t xb = jb < d ? L[jb] : INT32_MAX;
+      int pa, pb;
+      count_below2(stage, cl, top, xa, xb, pa, pb);
+      const bool fa = ja < d && pa < cl && stage[pa] == xa;
+      const bool fb = jb < d && pb < cl && stage[pb] == xb;
+      const unsigned ma = __ballot_sync(kFull, fa), mb = __ballot_sync(kFull, fb);
+      if (lane == 0) {
+        if (ma) atomicOr(Ri + q0, ma);
+        if (mb && q0 + 1 < w_d) atomicOr(Ri + q0 + 1, mb);
+      }
+      if (ETRI) {
+        if (fa) on_hit(ja, rsi + c0 + pa);
+        if (fb) on_hit(jb, rsi + c0 + pb);
+      }
+    }
+  }
+  __syncwarp();
+}
+
 // Position of the r-th set bit (r counted from 0) of the W-word row.
 __device__ __forceinline__ int select_bit(const uint32_t* row, int W, int r) {
   for (int q = 0; q < W; ++q) {
@@ -320,6 +364,7 @@ struct WarpSmem {
   eid_t rs[kWarpMaxDeg];
   uint32_t R[kWarpMaxDeg * kWarpW];
   int colcnt[kWarpMaxDeg];  // edge-triangle mode: rows with bit j set
+  vid_t stage[kStage];      // a long row, staged to look the root's list up in it
 };
 
 template <int K, bool STATS, bool ETRI, bool PAIRS = false, bool TT = false>
@@ -396,6 +441,15 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
       const int len = ws.deg[i];
       if (len < kLongRow) continue;
       const eid_t rsi = ws.rs[i];
+      if (len > d) {  // the row is the longer list: look the root's list up in it
+        flip_row<ETRI>(col, rsi, len, ws.L, d, w_d, ws.R + i * w_d, ws.stage,
+                       [&](int j, eid_t e) {
+                         const unsigned o = atomicAdd(tri + e, 1u);
+                         if (PAIRS) pairs += (acc_t)o;
+                         atomicAdd(&ws.colcnt[j], 1);
+                       });
+        continue;
+      }
       for (int t0 = lane; t0 < len; t0 += 64) {
         const bool two = t0 + 32 < len;
         const int t1 = two ? t0 + 32 : t0;

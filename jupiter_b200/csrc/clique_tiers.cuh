@@ -112,8 +112,10 @@ __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
 }
 
 // ------------------------------------------------------------------ warp tier (d <= 128)
+// The warp tier's shared memory (8 x WarpSmem, 49 KB) allows four CTAs per SM, so its
+// register budget is that of four CTAs.
 template <int K, bool STATS, bool ETRI = false, bool PAIRS = false, bool TT = false>
-__global__ void __launch_bounds__(256) k_clique_warp(CliqueArgs a) {
+__global__ void __launch_bounds__(256, 4) k_clique_warp(CliqueArgs a) {
   extern __shared__ __align__(16) unsigned char wsmem[];
   WarpSmem& ws = reinterpret_cast<WarpSmem*>(wsmem)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
