@@ -214,6 +214,9 @@ typedef struct {
                              apexes 1/8x) */
   int32_t intersect;      /* last clique level on edge-rooted lists: 0 searches the keys of
                              the shorter list in the longer one, 1 always the candidates */
+  int32_t graphs;         /* 1: a batch's launches (table copies, the one to three persistent
+                             kernels, the count read-back) are captured in a CUDA graph and
+                             replayed while the launch plan is unchanged; 0: launched directly */
 } jgpm_tuning;
 
 typedef struct {

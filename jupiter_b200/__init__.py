@@ -72,7 +72,8 @@ class _Job(ctypes.Structure):
 class Tuning(ctypes.Structure):
     """Work-split knobs of the batched (and plain clique) kernels."""
     _fields_ = [("min_group", ctypes.c_int32), ("split_degree", ctypes.c_int32),
-                ("roots_per_task", ctypes.c_int32), ("intersect", ctypes.c_int32)]
+                ("roots_per_task", ctypes.c_int32), ("intersect", ctypes.c_int32),
+                ("graphs", ctypes.c_int32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

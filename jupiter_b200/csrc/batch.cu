@@ -597,13 +597,98 @@ int build_tasks(const std::vector<BatchJobIn>& in, const jgpm_tuning& tu, BatchC
 
 }  // namespace
 
+// The stream operations of one batch: table uploads, counter resets, the large 4-cycle apex
+// kernel, the task kernel, the lane-group kernel and the count read-back, in that order.
+cudaError_t enqueue_plan(const LaunchPlan& p, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  auto ok = [&](cudaError_t r) {
+    if (e == cudaSuccess) e = r;
+  };
+  if (p.tri_bytes) ok(cudaMemsetAsync(p.d_tri, 0, p.tri_bytes, s));
+  ok(cudaMemcpyAsync(p.d_jobs, p.h_jobs, p.jobs_bytes, cudaMemcpyHostToDevice, s));
+  if (p.tasks_bytes)
+    ok(cudaMemcpyAsync(p.d_tasks, p.h_tasks, p.tasks_bytes, cudaMemcpyHostToDevice, s));
+  ok(cudaMemsetAsync(p.d_counts, 0, p.counts_bytes, s));
+  ok(cudaMemsetAsync(p.d_cursor, 0, 3 * sizeof(unsigned long long), s));
+  if (p.c4_kernel) {
+    if (p.c4_zero_bytes) ok(cudaMemsetAsync(p.d_c4_zero, 0, p.c4_zero_bytes, s));
+    ok(cudaMemcpyAsync(p.d_c4_tasks, p.h_c4_tasks, p.c4_tasks_bytes, cudaMemcpyHostToDevice, s));
+    C4BatchArgs b;
+    memcpy(&b, p.c4_args, sizeof(b));
+    if (p.c4_kernel == kC4NarrowThreads)
+      k_batch_c4_large<kC4NarrowThreads><<<p.c4_ctas, kC4NarrowThreads, p.c4_smem, s>>>(b);
+    else
+      k_batch_c4_large<kC4WideThreads><<<p.c4_ctas, kC4WideThreads, p.c4_smem, s>>>(b);
+    ok(cudaGetLastError());
+  }
+  BatchArgs a;
+  memcpy(&a, p.args, sizeof(a));
+  if (p.main_grid) k_batch<<<p.main_grid, 256, p.main_smem, s>>>(a);
+  if (p.groups_grid) k_batch_groups<<<p.groups_grid, 256, 0, s>>>(a);
+  ok(cudaGetLastError());
+  if (p.h_counts)
+    ok(cudaMemcpyAsync(p.h_counts, p.d_counts, p.d2h_bytes, cudaMemcpyDeviceToHost, s));
+  return e;
+}
+
+// Issues the plan on `s`: replays the context's captured graph when the plan is unchanged,
+// else captures the operations into a graph (updating the executable graph in place when its
+// topology allows, instantiating a new one otherwise) and launches it.
+int launch_plan(BatchCtx& c, const LaunchPlan& p, cudaStream_t s, bool use_graph) {
+  if (!use_graph) {
+    const cudaError_t e = enqueue_plan(p, s);
+    if (e != cudaSuccess) {
+      jgpm_set_error_(std::string("batch launch: ") + cudaGetErrorString(e));
+      return JGPM_ECUDA;
+    }
+    return JGPM_OK;
+  }
+  if (!(c.exec && c.have_plan && memcmp(&p, &c.plan, sizeof(LaunchPlan)) == 0)) {
+    cudaGraph_t g = nullptr;
+    JGPM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t e = enqueue_plan(p, s);
+    const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      jgpm_set_error_(std::string("batch graph capture: ") +
+                      cudaGetErrorString(e != cudaSuccess ? e : e2));
+      return JGPM_ECUDA;
+    }
+    if (c.exec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(c.exec, g, &info) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(c.exec);
+        c.exec = nullptr;
+      }
+    }
+    if (!c.exec) {
+      const cudaError_t ei = cudaGraphInstantiate(&c.exec, g, 0);
+      if (ei != cudaSuccess) {
+        c.exec = nullptr;
+        cudaGraphDestroy(g);
+        jgpm_set_error_(std::string("batch graph instantiate: ") + cudaGetErrorString(ei));
+        return JGPM_ECUDA;
+      }
+    }
+    cudaGraphDestroy(g);
+    c.plan = p;
+    c.have_plan = true;
+  }
+  JGPM_CUDA_TRY(cudaGraphLaunch(c.exec, s));
+  return JGPM_OK;
+}
+
 // Enqueues one batched launch on `s`; per-job counts land in c.counts (device) and are
-// copied to `h_counts` (pinned or pageable host memory) on the same stream.
+// copied to `h_counts` (pinned host memory, or null: the context's pinned buffer) on the same
+// stream.  All allocation and kernel set-up happens before the stream operations, which are
+// replayed from a CUDA graph while the launch plan repeats (tu.graphs).
 int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tuning& tu,
                   cudaStream_t s, uint64_t* h_counts, int* ntasks_out, int* launches_out) {
   BuildOut o;
   int rc;
-  if ((rc = build_tasks(in, tu, c, &o))) return rc;
+  if ((rc = build_tasks(in, tu, c, &o))) return rc;  // waits for this context's last batch
   const int sms = device_sm_count(c.device);
   const int W = (o.dmax + 31) / 32;
   const int wW = (o.wdmax + 31) / 32;
@@ -618,14 +703,23 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   if ((rc = c.tasks.reserve(std::max<size_t>(1, nt) * sizeof(Task)))) return rc;
   if ((rc = c.counts.reserve(nj * sizeof(unsigned long long)))) return rc;
   if ((rc = c.cursor.reserve(3 * sizeof(unsigned long long)))) return rc;
+  if ((rc = c.h_jobs_pin.reserve(nj * sizeof(JobDesc)))) return rc;
+  if (!h_counts) {
+    if ((rc = c.h_counts_pin.reserve(nj * sizeof(uint64_t)))) return rc;
+    h_counts = (uint64_t*)c.h_counts_pin.p;
+  }
+  LaunchPlan p;
+  memset(&p, 0, sizeof(p));
   if (o.tri_bytes) {
     if ((rc = c.tri.reserve(o.tri_bytes))) return rc;
     for (size_t ji = 0; ji < nj; ++ji)
       if (c.h_jobs[ji].kind == kJobDiamond || c.h_jobs[ji].kind == kJobIndTT)
         c.h_jobs[ji].tri = (uint32_t*)((char*)c.tri.p + c.tri_off[ji]);
-    JGPM_CUDA_TRY(cudaMemsetAsync(c.tri.p, 0, o.tri_bytes, s));
+    p.d_tri = c.tri.p;
+    p.tri_bytes = o.tri_bytes;
   }
-  BatchArgs a{};
+  BatchArgs a;
+  memset(&a, 0, sizeof(a));
   if (o.wdmax > 0) {
     if ((rc = c.rows.reserve((size_t)grid * o.wdmax * wW * sizeof(uint32_t)))) return rc;
     a.rows = (uint32_t*)c.rows.p;
@@ -638,14 +732,16 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
       return rc;
     a.list_scratch = (int32_t*)c.lists.p;
   }
-  JGPM_CUDA_TRY(cudaMemcpyAsync(c.jobs.p, c.h_jobs.data(), nj * sizeof(JobDesc),
-                                cudaMemcpyHostToDevice, s));
-  if (nt)
-    JGPM_CUDA_TRY(cudaMemcpyAsync(c.tasks.p, c.h_tasks.p, nt * sizeof(Task),
-                                  cudaMemcpyHostToDevice, s));
-  if ((rc = c.h_tasks.record(s))) return rc;
-  JGPM_CUDA_TRY(cudaMemsetAsync(c.counts.p, 0, nj * sizeof(unsigned long long), s));
-  JGPM_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, 3 * sizeof(unsigned long long), s));
+  memcpy(c.h_jobs_pin.p, c.h_jobs.data(), nj * sizeof(JobDesc));
+  p.d_jobs = c.jobs.p;
+  p.h_jobs = c.h_jobs_pin.p;
+  p.jobs_bytes = nj * sizeof(JobDesc);
+  p.d_tasks = c.tasks.p;
+  p.h_tasks = c.h_tasks.p;
+  p.tasks_bytes = nt * sizeof(Task);
+  p.d_counts = c.counts.p;
+  p.counts_bytes = nj * sizeof(unsigned long long);
+  p.d_cursor = c.cursor.p;
   // large 4-cycle apexes: k_batch_c4_large on the same stream, before k_batch.  (Run side by
   // side on two streams the two kernels took twice their sum: the persistent k_batch CTAs hold
   // the SMs whose shared memory the slab CTAs need, and the two working sets share L2.)
@@ -669,15 +765,17 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     if (need) {
       if ((rc = c.c4.reserve(need))) return rc;
       if (c.c4_zeroed < need) {  // counters are zero between apexes; zero fresh memory once
-        JGPM_CUDA_TRY(cudaMemsetAsync(c.c4.p, 0, c.c4.bytes, s));
+        p.d_c4_zero = c.c4.p;
+        p.c4_zero_bytes = c.c4.bytes;
         c.c4_zeroed = c.c4.bytes;
       }
       if ((rc = c.c4t.reserve(need))) return rc;
     }
     if ((rc = c.c4_tasks.reserve(n4 * sizeof(Task)))) return rc;
-    JGPM_CUDA_TRY(cudaMemcpyAsync(c.c4_tasks.p, c.h_c4_tasks.data(), n4 * sizeof(Task),
-                                  cudaMemcpyHostToDevice, s));
-    C4BatchArgs b{};
+    if ((rc = c.h_c4_pin.reserve(n4 * sizeof(Task)))) return rc;
+    memcpy(c.h_c4_pin.p, c.h_c4_tasks.data(), n4 * sizeof(Task));
+    C4BatchArgs b;
+    memset(&b, 0, sizeof(b));
     b.jobs = (const JobDesc*)c.jobs.p;
     b.tasks = (const Task*)c.c4_tasks.p;
     b.ntasks = (int64_t)n4;
@@ -687,8 +785,14 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
     b.touched = need ? (vid_t*)c.c4t.p : nullptr;
     b.stride = o.c4max;
     b.words = form.words;
-    kern<<<(int)ctas, form.threads, slab_bytes, s>>>(b);
-    JGPM_CUDA_TRY(cudaGetLastError());
+    static_assert(sizeof(C4BatchArgs) <= sizeof(p.c4_args), "plan: C4BatchArgs too large");
+    memcpy(p.c4_args, &b, sizeof(b));
+    p.c4_kernel = form.threads;
+    p.c4_ctas = (int)ctas;
+    p.c4_smem = slab_bytes;
+    p.d_c4_tasks = c.c4_tasks.p;
+    p.h_c4_tasks = c.h_c4_pin.p;
+    p.c4_tasks_bytes = n4 * sizeof(Task);
   }
   a.jobs = (const JobDesc*)c.jobs.p;
   a.tasks = (const Task*)c.tasks.p;
@@ -700,20 +804,22 @@ int batch_enqueue(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   a.intersect = tu.intersect;
   const int64_t nmain = c.nmain;
   a.nmain = nmain;
-  if (nmain) k_batch<<<grid, 256, smem, s>>>(a);
-  int glaunch = 0;
+  static_assert(sizeof(BatchArgs) <= sizeof(p.args), "plan: BatchArgs too large");
+  memcpy(p.args, &a, sizeof(a));
+  p.main_grid = nmain ? grid : 0;
+  p.main_smem = smem;
   if ((int64_t)nt > nmain) {
     int gper = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&gper, k_batch_groups, 256, 0);
-    k_batch_groups<<<sms * std::max(1, gper), 256, 0, s>>>(a);
-    glaunch = 1;
+    p.groups_grid = sms * std::max(1, gper);
   }
-  JGPM_CUDA_TRY(cudaGetLastError());
-  if (h_counts)
-    JGPM_CUDA_TRY(cudaMemcpyAsync(h_counts, c.counts.p, nj * sizeof(uint64_t),
-                                  cudaMemcpyDeviceToHost, s));
+  p.h_counts = h_counts;
+  p.d2h_bytes = nj * sizeof(uint64_t);
+  if ((rc = launch_plan(c, p, s, tu.graphs != 0))) return rc;
+  // the pinned tables may be rewritten once this batch has finished
+  if ((rc = c.h_tasks.record(s))) return rc;
   if (ntasks_out) *ntasks_out = (int)(nt + n4);
-  if (launches_out) *launches_out = (nmain ? 1 : 0) + glaunch + (n4 ? 1 : 0);
+  if (launches_out) *launches_out = (nmain ? 1 : 0) + (p.groups_grid ? 1 : 0) + (n4 ? 1 : 0);
   return JGPM_OK;
 }
 
@@ -742,6 +848,7 @@ jgpm_tuning default_tuning() {
   t.split_degree = 128;
   t.roots_per_task = 256;
   t.intersect = 0;
+  t.graphs = 1;
   return t;
 }
 
@@ -785,9 +892,10 @@ double time_batch(BatchCtx& c, const std::vector<BatchJobIn>& in, const jgpm_tun
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, s);
-  int rc = batch_enqueue(c, in, tu, s, counts.data(), nullptr);
+  int rc = batch_enqueue(c, in, tu, s, nullptr, nullptr);
   cudaEventRecord(e1, s);
   if (rc == JGPM_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = JGPM_ECUDA;
+  if (rc == JGPM_OK) memcpy(counts.data(), c.h_counts_pin.p, counts.size() * sizeof(uint64_t));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
@@ -830,7 +938,7 @@ int jgpm_batch_count(const jgpm_job* jobs, int32_t njobs, const jgpm_tuning* tun
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, s);
-  rc = batch_enqueue(c, in, tu, s, h.data(), &ntasks, &launches);
+  rc = batch_enqueue(c, in, tu, s, nullptr, &ntasks, &launches);
   cudaEventRecord(e1, s);
   cudaError_t ce = cudaStreamSynchronize(s);
   float ms = 0.f;
@@ -843,7 +951,7 @@ int jgpm_batch_count(const jgpm_job* jobs, int32_t njobs, const jgpm_tuning* tun
     jgpm_set_error_(std::string("jgpm_batch_count: ") + cudaGetErrorString(ce));
     return JGPM_ECUDA;
   }
-  memcpy(counts, h.data(), h.size() * sizeof(uint64_t));
+  memcpy(counts, c.h_counts_pin.p, h.size() * sizeof(uint64_t));
   if (st) {
     st->kernel_ms = ms;
     st->launches = launches;

@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "jgpm_internal.h"
@@ -136,8 +138,68 @@ struct PinnedTasks {
 
 // Reusable per-device launch state of the batched kernel (task/job tables, counters,
 // scratch).  One per server slot or per synchronous caller.
+// Pinned host staging reused across batches (written only after the previous batch of the
+// same context has finished).
+struct PinnedBytes {
+  void* p = nullptr;
+  size_t cap = 0;
+  int reserve(size_t want) {
+    if (want <= cap) return JGPM_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    const size_t sz = std::max<size_t>(want + want / 4, 4096);
+    if (cudaHostAlloc(&p, sz, cudaHostAllocDefault) != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      jgpm_set_error_("batch: pinned host allocation failed");
+      return JGPM_ENOMEM;
+    }
+    cap = sz;
+    return JGPM_OK;
+  }
+  ~PinnedBytes() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+// Everything the stream operations of one batch need, as plain data: two batches with equal
+// plans (bytewise) issue identical operations, so a captured CUDA graph can be replayed.
+struct LaunchPlan {
+  void* d_jobs;
+  const void* h_jobs;
+  size_t jobs_bytes;
+  void* d_tasks;
+  const void* h_tasks;
+  size_t tasks_bytes;
+  void* d_c4_tasks;
+  const void* h_c4_tasks;
+  size_t c4_tasks_bytes;
+  void* d_tri;
+  size_t tri_bytes;
+  void* d_counts;
+  size_t counts_bytes;
+  void* d_cursor;
+  void* d_c4_zero;
+  size_t c4_zero_bytes;
+  int c4_kernel;  // 0 none, else the slab form's threads
+  int c4_ctas;
+  size_t c4_smem;
+  unsigned char c4_args[128];
+  int main_grid;
+  size_t main_smem;
+  int groups_grid;
+  unsigned char args[128];
+  void* h_counts;
+  size_t d2h_bytes;
+};
+
 struct BatchCtx {
   int device = 0;
+  PinnedBytes h_jobs_pin, h_c4_pin, h_counts_pin;
+  cudaGraphExec_t exec = nullptr;  // the captured launches of `plan`
+  LaunchPlan plan;
+  bool have_plan = false;
   DevArena jobs, tasks, counts, cursor, c4, c4t, lists, tri, rows, c4_tasks;
   std::vector<JobDesc> h_jobs;
   PinnedTasks h_tasks;           // the main queue
@@ -148,6 +210,7 @@ struct BatchCtx {
   size_t c4_zeroed = 0;
   size_t c4_cap_bytes = (size_t)4 << 30;  // memory cap of the 4-cycle counter arrays
   ~BatchCtx() {
+    if (exec) cudaGraphExecDestroy(exec);
     for (DevArena* d : {&jobs, &tasks, &counts, &cursor, &c4, &c4t, &lists, &tri, &rows,
                         &c4_tasks})
       if (d->p) cudaFree(d->p);

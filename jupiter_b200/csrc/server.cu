@@ -2,8 +2,12 @@
 //
 // A scheduler thread owns `max_inflight` slots (a stream, a batched-kernel context and a
 // pinned count buffer each).  Whenever a slot is free and queries are pending, it packs up to
-// `max_batch` admissible queries (FIFO) into one batched persistent launch on that slot's
-// stream and moves on; completions are detected with events, so batches of queries that
+// `max_batch` admissible queries into one batched persistent launch on that slot's stream and
+// moves on.  Queries are taken shortest estimated work first, with aging: a query's estimate
+// is the running average of the service times measured for its (graph, pattern), or before
+// the first one a prior of DAG arcs x a per-pattern factor, and its priority is that estimate
+// minus kAging x its wait, so light queries do not queue behind heavy ones and a heavy one is
+// not passed over for ever; completions are detected with events, so batches of queries that
 // arrived while others run overlap on the device.  Admission: a query's graph must be
 // resident (the pool uploads it again, evicting least-recently-used idle graphs, if needed)
 // and the resident graph bytes plus the estimated frontier memory of everything in flight
@@ -40,6 +44,7 @@ using Clock = std::chrono::steady_clock;
 
 constexpr int kPlainWorkers = 2;
 constexpr int64_t kHeavyArcs = (int64_t)16 << 20;  // DAG arcs (symmetric arcs / 2)
+constexpr double kAging = 0.1;  // seconds of estimated work forgiven per second of waiting
 
 double now_s() {
   return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
@@ -58,6 +63,8 @@ struct Query {
   bool plain = false;   // not batchable: runs through jgpm_count on the plain lane
   int induced = 0;
   std::string pattern;
+  std::string cost_key;  // pattern as submitted (with the "induced:" prefix)
+  double est = 0.0;      // estimated service time (s)
 };
 
 struct PoolGraph {
@@ -78,6 +85,7 @@ struct Slot {
   uint64_t* h_counts = nullptr;  // pinned
   std::vector<std::shared_ptr<Query>> queries;
   uint64_t frontier = 0;  // of the batch in flight
+  double t_launch = 0.0;
   bool busy = false;
 };
 
@@ -104,10 +112,52 @@ struct jgpm_server {
   uint64_t inflight_frontier = 0;
   jgpm_server_stats st{};
   std::string sched_error;
+  // measured service time (s) per (graph, pattern): the scheduler's work estimates
+  std::unordered_map<std::string, double> cost;
 };
 
 namespace jgpm {
 namespace {
+
+std::string cost_id(int32_t graph_id, const std::string& pattern) {
+  return std::to_string(graph_id) + "/" + pattern;
+}
+
+// Prior service time of a query before any has been measured: DAG arcs x a per-pattern
+// factor (seconds per arc; measured ratios of the plain kernels on R-MAT graphs).
+double prior_cost(const jgpm_graph* g, const std::string& pattern) {
+  const double arcs = (double)(g->m_dag > 0 ? g->m_dag : g->m / 2);
+  double f = 2.0;  // literal plans and census pieces
+  if (pattern == "triangle" || pattern == "P0" || pattern == "3-clique") f = 0.1;
+  else if (pattern == "4-clique" || pattern == "P13") f = 0.45;
+  else if (pattern == "5-clique" || pattern == "P14") f = 1.0;
+  else if (pattern == "diamond" || pattern == "P2") f = 0.5;
+  else if (pattern == "induced:tailed-triangle") f = 0.55;
+  else if (pattern == "4-cycle" || pattern == "P1") f = 3.0;
+  return arcs * f * 1e-9;
+}
+
+// Folds a measured service time into the running average of its (graph, pattern) (mu held).
+void learn_cost(jgpm_server* s, const Query& q, double seconds) {
+  const std::string id = cost_id(q.graph_id, q.cost_key);
+  auto it = s->cost.find(id);
+  if (it == s->cost.end()) s->cost.emplace(id, seconds);
+  else it->second = 0.5 * it->second + 0.5 * seconds;
+}
+
+// Priority of a pending query (lower first): estimated work, less credit for waiting.
+double priority(const Query& q, double now) { return q.est - kAging * (now - q.t_submit); }
+
+// Indices of `pending` in priority order.
+std::vector<size_t> by_priority(const std::deque<std::shared_ptr<Query>>& pending) {
+  const double now = now_s();
+  std::vector<std::pair<double, size_t>> k(pending.size());
+  for (size_t i = 0; i < pending.size(); ++i) k[i] = {priority(*pending[i], now), i};
+  std::stable_sort(k.begin(), k.end());
+  std::vector<size_t> out(k.size());
+  for (size_t i = 0; i < k.size(); ++i) out[i] = k[i].second;
+  return out;
+}
 
 bool over_budget(jgpm_server* s, uint64_t extra) {
   return s->resident_bytes + s->inflight_frontier + extra > s->cfg.memory_budget_bytes;
@@ -146,35 +196,36 @@ int launch_batch(jgpm_server* s, Slot& slot) {
   std::vector<std::shared_ptr<Query>> batch;
   std::vector<BatchJobIn> in;
   uint64_t own = 0, shared = 0;
-  for (auto it = s->pending.begin(); it != s->pending.end() && (int)batch.size() < s->cfg.max_batch;) {
-    std::shared_ptr<Query> q = *it;
+  std::vector<bool> taken(s->pending.size(), false);
+  for (size_t idx : by_priority(s->pending)) {
+    if ((int)batch.size() >= s->cfg.max_batch) break;
+    std::shared_ptr<Query> q = s->pending[idx];
     PoolGraph& pg = s->graphs[q->graph_id];
-    if (pg.plain_busy) {  // the graph is in a plain-lane query: next launch
-      ++it;
-      continue;
-    }
+    if (pg.plain_busy) continue;  // the graph is in a plain-lane query: next launch
     const uint64_t with_q = own + q->fr_own + std::max(shared, q->fr_shared);
     if (!pg.resident) {
       int rc = make_resident(s, q->graph_id, with_q);
-      if (rc == JGPM_EBUSY) {
-        ++it;
-        continue;
-      }
+      if (rc == JGPM_EBUSY) continue;
       if (rc) return rc;
     }
-    if (over_budget(s, with_q) && (!batch.empty() || s->inflight_frontier > 0)) {
-      ++it;  // wait for in-flight work to release memory
-      continue;
-    }
+    if (over_budget(s, with_q) && (!batch.empty() || s->inflight_frontier > 0))
+      continue;  // wait for in-flight work to release memory
     own += q->fr_own;
     shared = std::max(shared, q->fr_shared);
     pg.inflight++;
     pg.last_use = ++s->use_clock;
     in.push_back(BatchJobIn{pg.g, q->kind, q->k});
     batch.push_back(q);
-    it = s->pending.erase(it);
+    taken[idx] = true;
   }
   if (batch.empty()) return JGPM_OK;
+  {
+    std::deque<std::shared_ptr<Query>> rest;
+    for (size_t i = 0; i < s->pending.size(); ++i)
+      if (!taken[i]) rest.push_back(s->pending[i]);
+    s->pending.swap(rest);
+  }
+  slot.t_launch = now_s();
   int ntasks = 0;
   int rc = batch_enqueue(slot.ctx, in, s->cfg.tuning, slot.stream, slot.h_counts, &ntasks);
   if (rc) {
@@ -198,6 +249,9 @@ int launch_batch(jgpm_server* s, Slot& slot) {
 
 void complete_slot(jgpm_server* s, Slot& slot) {
   const double t = now_s();
+  // the batch's service time, shared out over its queries by their estimates
+  double est_sum = 0.0;
+  for (auto& qp : slot.queries) est_sum += qp->est;
   for (size_t i = 0; i < slot.queries.size(); ++i) {
     Query& q = *slot.queries[i];
     q.count = slot.h_counts[i];
@@ -205,6 +259,7 @@ void complete_slot(jgpm_server* s, Slot& slot) {
     q.status = 0;
     s->graphs[q.graph_id].inflight--;
     s->st.completed++;
+    if (est_sum > 0.0) learn_cost(s, q, (t - slot.t_launch) * q.est / est_sum);
   }
   // derived structures (DAG, tiers, 4-cycle classes) may have grown the graphs
   for (auto& qp : slot.queries) {
@@ -266,11 +321,16 @@ void plain_worker(jgpm_server* s) {
       s->cv_plain.wait_for(lk, std::chrono::milliseconds(50));
       continue;
     }
-    // the first pending query whose graph no batch or other plain query is using
-    auto pick = s->plain_pending.begin();
-    while (pick != s->plain_pending.end() && (s->graphs[(*pick)->graph_id].inflight > 0 ||
-                                              s->graphs[(*pick)->graph_id].plain_busy))
-      ++pick;
+    // the first pending query, in priority order, whose graph no batch or other plain query
+    // is using
+    auto pick = s->plain_pending.end();
+    for (size_t idx : by_priority(s->plain_pending)) {
+      const PoolGraph& c = s->graphs[s->plain_pending[idx]->graph_id];
+      if (c.inflight == 0 && !c.plain_busy) {
+        pick = s->plain_pending.begin() + (std::ptrdiff_t)idx;
+        break;
+      }
+    }
     if (pick == s->plain_pending.end()) {
       s->cv_plain.wait_for(lk, std::chrono::microseconds(200));
       continue;
@@ -303,6 +363,7 @@ void plain_worker(jgpm_server* s) {
     jgpm_graph* g = pg.g;
     lk.unlock();
     uint64_t cnt = 0;
+    const double t_start = now_s();
     const int rc = jgpm_count_ex(g, q->pattern.c_str(), q->induced, 1, 0u, &cnt, nullptr);
     const std::string err = rc ? std::string(jgpm_last_error()) : std::string();
     lk.lock();
@@ -319,7 +380,10 @@ void plain_worker(jgpm_server* s) {
     q->t_done = now_s();
     q->status = rc;
     if (rc) s->sched_error = err;
-    else s->st.completed++;
+    else {
+      s->st.completed++;
+      learn_cost(s, *q, q->t_done - t_start);
+    }
     s->cv_done.notify_all();
     s->cv_work.notify_one();  // the graph is free for batches again
   }
@@ -509,6 +573,11 @@ int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, ui
     q->frontier += count_scratch_bytes(g, qp, q->induced);
   } else {
     estimate_frontier(s, g, q->kind, &q->fr_own, &q->fr_shared);
+  }
+  q->cost_key = p;
+  {
+    auto it = s->cost.find(cost_id(graph_id, p));
+    q->est = it != s->cost.end() ? it->second : prior_cost(g, p);
   }
   const uint64_t need = q->plain ? q->frontier : q->fr_own + q->fr_shared;
   if (need + s->graphs[graph_id].bytes > s->cfg.memory_budget_bytes) {

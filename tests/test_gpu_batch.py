@@ -67,6 +67,23 @@ def test_each_job_same_alone_and_in_mix(gpu, mixed):
         assert c == want[(gs.index(g), p)]
 
 
+def test_graph_replay_and_direct_launches_agree(gpu, mixed):
+    """A batch's launches are captured in a CUDA graph and replayed while its launch plan
+    repeats; a changed job set recaptures (updating the executable graph in place).  Replayed,
+    recaptured and directly launched batches give the oracle's counts."""
+    specs, gs, want = mixed
+    sets = [[(g, p) for g in gs for p in PATTERNS],
+            [(g, p) for g in gs[:5] for p in ("triangle", "4-cycle")],
+            [(g, "diamond") for g in gs[3:9]]]
+    for jobs in sets + sets[:1]:
+        for graphs in (1, 1, 0):  # capture (or update), replay, direct
+            t = gpu.Tuning(8, 128, 256, 0, graphs)
+            counts, st = gpu.batch_count(jobs, t)
+            assert st["tuning"]["graphs"] == graphs
+            for (g, p), c in zip(jobs, counts):
+                assert c == want[(gs.index(g), p)], (gs.index(g), p, graphs)
+
+
 @pytest.mark.parametrize("min_group,split,rpt,isect",
                          list(itertools.product([4, 8, 32], [32, 128], [8, 256], [0, 1])))
 def test_every_tuning_gives_the_same_counts(gpu, mixed, min_group, split, rpt, isect):
