@@ -458,10 +458,17 @@ def run_batched(args):
     plain_counts = [g.count(p) for g, p in jobs]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    plain_dev_ms = 0.0
     for _ in range(args.plain_passes):
-        plain_counts = [g.count(p) for g, p in jobs]
+        res = [g.count(p, details=True) for g, p in jobs]
+        plain_counts = [c for c, _ in res]
+        plain_dev_ms += sum(st["kernel_ms"] for _, st in res)
     torch.cuda.synchronize()
     plain_s = (time.perf_counter() - t0) / args.plain_passes
+    plain_dev_s = plain_dev_ms / 1e3 / args.plain_passes
+    # plain device time of the jobs that take at least a millisecond of device time alone: their
+    # launches fill the GPU, so batching can remove little of it
+    big_dev_s = sum(st["kernel_ms"] for _, st in res if st["kernel_ms"] >= 1.0) / 1e3
     tuning = J.autotune(jobs, sample_jobs=256)
     for _ in range(args.warmup):
         J.batch_count(jobs, tuning)
@@ -492,7 +499,14 @@ def run_batched(args):
            "speedup_vs_plain": (len(jobs) / (dev_ms / 1e3)) / (len(jobs) / plain_s),
            "speedup_vs_plain_wall": plain_s / wall,
            "counts_identical_to_plain": True, "graph_generation_s": gen_s,
-           "gpu_launches": launches}
+           "gpu_launches": launches,
+           "amdahl": {"plain_wall_s": plain_s, "plain_device_s": plain_dev_s,
+                      "plain_host_share": 1.0 - plain_dev_s / plain_s,
+                      "plain_device_s_in_jobs_of_1ms_or_more": big_dev_s,
+                      "bound_if_batching_removed_all_host_time": plain_s / plain_dev_s,
+                      "batched_vs_plain_device": plain_dev_s / (dev_ms / 1e3),
+                      "note": "the batch can remove the plain calls' host time and the tails "
+                              "of small launches, not the device work of jobs that fill the GPU"}}
     for g in graphs:
         g.close()
     print(json.dumps(out), flush=True)

@@ -211,14 +211,13 @@ int ensure_c4_apexes(jgpm_graph* g) {
   JGPM_CUDA_TRY(cudaStreamSynchronize(s));
   const int64_t nsmall = (int64_t)h[0], nlarge = (int64_t)h[1], nmid = (int64_t)h[2];
   int32_t *ds = nullptr, *dm = nullptr, *dl = nullptr;
-  if (cudaMalloc(&ds, std::max<int64_t>(1, nsmall) * 4) != cudaSuccess ||
-      cudaMalloc(&dm, std::max<int64_t>(1, nmid) * 4) != cudaSuccess ||
-      cudaMalloc(&dl, std::max<int64_t>(1, 2 * nlarge) * 4) != cudaSuccess) {
-    cudaGetLastError();
-    cudaFree(ds);
-    cudaFree(dm);
-    jgpm_set_error_("4-cycle: device allocation failed");
-    return JGPM_ENOMEM;
+  int arc = gmalloc((void**)&ds, std::max<int64_t>(1, nsmall) * 4, s);
+  if (!arc) arc = gmalloc((void**)&dm, std::max<int64_t>(1, nmid) * 4, s);
+  if (!arc) arc = gmalloc((void**)&dl, std::max<int64_t>(1, 2 * nlarge) * 4, s);
+  if (arc) {
+    gfree(ds, s);
+    gfree(dm, s);
+    return arc;
   }
   g->d_c4_small = ds;
   g->d_c4_mid = dm;

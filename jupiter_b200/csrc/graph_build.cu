@@ -184,6 +184,60 @@ __global__ void k_root_keys(const int64_t* dag_rowptr, int32_t n, int min_deg, u
   }
 }
 
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+
+// The library's pool on `dev`: it keeps every byte freed into it (no release threshold), so
+// repeated graph life cycles reuse the same memory.  Callers that need the memory elsewhere
+// get it back by the trim on an allocation failure.
+cudaMemPool_t device_pool(int dev) {
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pools[dev] = pool;
+  }
+  return g_pools[dev];
+}
+
+// Pinned host mirrors of the graphs' control blocks: slots of pinned slabs, reused.
+std::mutex g_ctl_mu;
+std::vector<DevControl*> g_ctl_free;
+
+DevControl* ctl_slot() {
+  std::lock_guard<std::mutex> lk(g_ctl_mu);
+  if (g_ctl_free.empty()) {
+    constexpr int kSlots = 256;
+    DevControl* slab = nullptr;
+    if (cudaMallocHost((void**)&slab, kSlots * sizeof(DevControl)) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    for (int i = kSlots - 1; i >= 0; --i) g_ctl_free.push_back(slab + i);
+  }
+  DevControl* p = g_ctl_free.back();
+  g_ctl_free.pop_back();
+  return p;
+}
+
+void ctl_release(DevControl* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_ctl_mu);
+  g_ctl_free.push_back(p);
+}
+
 int grid_for(int64_t work, int threads = 256) {
   int64_t b = (work + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -191,21 +245,47 @@ int grid_for(int64_t work, int threads = 256) {
   return (int)b;
 }
 
-template <typename T>
-int dalloc(T** p, size_t count) {
-  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+}  // namespace
+
+int gmalloc(void** p, size_t bytes, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaMemPool_t pool = device_pool(dev);
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaErrorMemoryAllocation;
+  if (e == cudaErrorMemoryAllocation && pool) {  // return the cached memory, then retry once
+    cudaGetLastError();
+    cudaDeviceSynchronize();
+    cudaMemPoolTrimTo(pool, 0);
+    e = cudaMallocFromPoolAsync(p, bytes, pool, s);
+  }
   if (e != cudaSuccess) {
-    jgpm_set_error_(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaGetLastError();
     *p = nullptr;
+    jgpm_set_error_(std::string("device allocation of ") + std::to_string(bytes) +
+                    " bytes: " + cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? JGPM_ENOMEM : JGPM_ECUDA;
   }
   return JGPM_OK;
 }
 
+void gfree(void* p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
+namespace {
+
+template <typename T>
+int dalloc(T** p, size_t count, cudaStream_t s) {
+  return gmalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T), s);
+}
+
+// A temporary device buffer, returned to the pool in the order of stream s.
 struct DevBuf {
+  cudaStream_t s;
   void* p = nullptr;
+  explicit DevBuf(cudaStream_t stream) : s(stream) {}
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (p) gfree(p, s);
   }
 };
 
@@ -213,21 +293,21 @@ struct DevBuf {
 int keys_to_csr(jgpm_graph* g, int32_t n, uint64_t* d_keys, int64_t nk, int shift,
                 uint64_t invalid, int end_bit) {
   cudaStream_t s = g->stream;
-  DevBuf alt, tmp, flags, pos;
+  DevBuf alt(g->stream), tmp(g->stream), flags(g->stream), pos(g->stream);
   int rc;
-  if ((rc = dalloc((uint64_t**)&alt.p, nk))) return rc;
+  if ((rc = dalloc((uint64_t**)&alt.p, nk, g->stream))) return rc;
   size_t tbytes = 0, tb2 = 0;
   cub::DoubleBuffer<uint64_t> db(d_keys, (uint64_t*)alt.p);
   JGPM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tbytes, db, nk, 0, end_bit, s));
   JGPM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb2, (int*)nullptr, (int64_t*)nullptr,
                                               nk, s));
   tbytes = std::max(tbytes, tb2);
-  if ((rc = dalloc((char**)&tmp.p, tbytes))) return rc;
+  if ((rc = dalloc((char**)&tmp.p, tbytes, g->stream))) return rc;
   JGPM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(tmp.p, tbytes, db, nk, 0, end_bit, s));
   uint64_t* sorted = db.Current();
   uint64_t* spare = db.Alternate();
-  if ((rc = dalloc((int**)&flags.p, nk))) return rc;
-  if ((rc = dalloc((int64_t**)&pos.p, nk + 1))) return rc;
+  if ((rc = dalloc((int**)&flags.p, nk, g->stream))) return rc;
+  if ((rc = dalloc((int64_t**)&pos.p, nk + 1, g->stream))) return rc;
   k_unique_flags<<<grid_for(nk), 256, 0, s>>>(sorted, nk, invalid, (int*)flags.p);
   JGPM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp.p, tbytes, (int*)flags.p, (int64_t*)pos.p,
                                               nk, s));
@@ -241,8 +321,8 @@ int keys_to_csr(jgpm_graph* g, int32_t n, uint64_t* d_keys, int64_t nk, int shif
     JGPM_CUDA_TRY(cudaStreamSynchronize(s));
   }
   const int64_t m = last_pos + last_flag;
-  if ((rc = dalloc(&g->d_col, m))) return rc;
-  if ((rc = dalloc(&g->d_rowptr, (size_t)n + 1))) return rc;
+  if ((rc = dalloc(&g->d_col, m, g->stream))) return rc;
+  if ((rc = dalloc(&g->d_rowptr, (size_t)n + 1, g->stream))) return rc;
   uint64_t* ukeys = spare;  // nk >= m entries, free after the sort
   k_compact_keys<<<grid_for(nk), 256, 0, s>>>(sorted, (int*)flags.p, (int64_t*)pos.p, nk,
                                               (1ull << shift) - 1, ukeys, g->d_col);
@@ -255,9 +335,9 @@ int keys_to_csr(jgpm_graph* g, int32_t n, uint64_t* d_keys, int64_t nk, int shif
 }
 
 int finish_sym(jgpm_graph* g) {
-  DevBuf md;
+  DevBuf md(g->stream);
   int rc;
-  if ((rc = dalloc((int**)&md.p, 1))) return rc;
+  if ((rc = dalloc((int**)&md.p, 1, g->stream))) return rc;
   JGPM_CUDA_TRY(cudaMemsetAsync(md.p, 0, sizeof(int), g->stream));
   k_max_degree<<<grid_for(g->n), 256, 0, g->stream>>>(g->d_rowptr, g->n, (int*)md.p);
   int h = 0;
@@ -312,9 +392,9 @@ int rmat_build(jgpm_graph* g, int64_t n, int64_t num_edges, double a, double b, 
   const uint64_t invalid = (uint64_t)n << shift;
   const int end_bit = 2 * shift;
   const int64_t nk = 2 * num_edges;
-  DevBuf keys;
+  DevBuf keys(g->stream);
   int rc;
-  if ((rc = dalloc((uint64_t**)&keys.p, nk))) return rc;
+  if ((rc = dalloc((uint64_t**)&keys.p, nk, g->stream))) return rc;
   k_rmat_keys<<<grid_for(num_edges), 256, 0, g->stream>>>(p, shift, (uint64_t*)keys.p, invalid);
   JGPM_CUDA_TRY(cudaGetLastError());
   if ((rc = keys_to_csr(g, (int32_t)n, (uint64_t*)keys.p, nk, shift, invalid, end_bit)))
@@ -329,12 +409,12 @@ int edges_build(jgpm_graph* g, const int32_t* src, const int32_t* dst, int64_t n
   }
   const int shift = shift_for(n);
   const uint64_t invalid = (uint64_t)n << shift;
-  DevBuf ds, dd, keys, bad;
+  DevBuf ds(g->stream), dd(g->stream), keys(g->stream), bad(g->stream);
   int rc;
-  if ((rc = dalloc((int32_t**)&ds.p, ne))) return rc;
-  if ((rc = dalloc((int32_t**)&dd.p, ne))) return rc;
-  if ((rc = dalloc((uint64_t**)&keys.p, 2 * ne))) return rc;
-  if ((rc = dalloc((int**)&bad.p, 1))) return rc;
+  if ((rc = dalloc((int32_t**)&ds.p, ne, g->stream))) return rc;
+  if ((rc = dalloc((int32_t**)&dd.p, ne, g->stream))) return rc;
+  if ((rc = dalloc((uint64_t**)&keys.p, 2 * ne, g->stream))) return rc;
+  if ((rc = dalloc((int**)&bad.p, 1, g->stream))) return rc;
   JGPM_CUDA_TRY(cudaMemcpyAsync(ds.p, src, ne * sizeof(int32_t), cudaMemcpyDefault, g->stream));
   JGPM_CUDA_TRY(cudaMemcpyAsync(dd.p, dst, ne * sizeof(int32_t), cudaMemcpyDefault, g->stream));
   JGPM_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), g->stream));
@@ -358,8 +438,8 @@ int upload_csr(jgpm_graph* g, const int64_t* rowptr, const int32_t* col, int32_t
     return JGPM_EINVAL;
   }
   int rc;
-  if ((rc = dalloc(&g->d_rowptr, (size_t)n + 1))) return rc;
-  if ((rc = dalloc(&g->d_col, m))) return rc;
+  if ((rc = dalloc(&g->d_rowptr, (size_t)n + 1, g->stream))) return rc;
+  if ((rc = dalloc(&g->d_col, m, g->stream))) return rc;
   JGPM_CUDA_TRY(cudaMemcpyAsync(g->d_rowptr, rowptr, ((size_t)n + 1) * sizeof(int64_t),
                                 cudaMemcpyDefault, g->stream));
   if (m > 0)
@@ -368,15 +448,15 @@ int upload_csr(jgpm_graph* g, const int64_t* rowptr, const int32_t* col, int32_t
   g->n = n;
   g->m = m;
   if (validate) {
-    DevBuf bad, src;
-    if ((rc = dalloc((int**)&bad.p, 1))) return rc;
+    DevBuf bad(g->stream), src(g->stream);
+    if ((rc = dalloc((int**)&bad.p, 1, g->stream))) return rc;
     JGPM_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), g->stream));
     k_rowptr_check<<<grid_for(n), 256, 0, g->stream>>>(g->d_rowptr, n, m, (int*)bad.p);
     int hbad = 0;
     JGPM_CUDA_TRY(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
     JGPM_CUDA_TRY(cudaStreamSynchronize(g->stream));
     if (!hbad && m > 0) {
-      if ((rc = dalloc((int32_t**)&src.p, m))) return rc;
+      if ((rc = dalloc((int32_t**)&src.p, m, g->stream))) return rc;
       k_arc_src<<<grid_for((int64_t)n * 32), 256, 0, g->stream>>>(g->d_rowptr, n,
                                                                   (int32_t*)src.p);
       k_validate<<<grid_for(m), 256, 0, g->stream>>>(g->d_rowptr, g->d_col, (int32_t*)src.p, n,
@@ -402,17 +482,17 @@ int ensure_dag(jgpm_graph* g) {
   const int64_t m = g->m;
   const int32_t n = g->n;
   int rc;
-  if ((rc = dalloc(&g->d_dag_rowptr, (size_t)n + 1))) return rc;
-  DevBuf src, keep, pos, tmp;
-  if ((rc = dalloc((int32_t**)&src.p, m))) return rc;
-  if ((rc = dalloc((int**)&keep.p, m))) return rc;
-  if ((rc = dalloc((int64_t**)&pos.p, m + 1))) return rc;
+  if ((rc = dalloc(&g->d_dag_rowptr, (size_t)n + 1, g->stream))) return rc;
+  DevBuf src(g->stream), keep(g->stream), pos(g->stream), tmp(g->stream);
+  if ((rc = dalloc((int32_t**)&src.p, m, g->stream))) return rc;
+  if ((rc = dalloc((int**)&keep.p, m, g->stream))) return rc;
+  if ((rc = dalloc((int64_t**)&pos.p, m + 1, g->stream))) return rc;
   k_arc_src<<<grid_for((int64_t)n * 32), 256, 0, s>>>(g->d_rowptr, n, (int32_t*)src.p);
   k_orient_flags<<<grid_for(m), 256, 0, s>>>(g->d_rowptr, g->d_col, (int32_t*)src.p, m,
                                              (int*)keep.p);
   size_t tb = 0;
   JGPM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, (int*)keep.p, (int64_t*)pos.p, m, s));
-  if ((rc = dalloc((char**)&tmp.p, tb))) return rc;
+  if ((rc = dalloc((char**)&tmp.p, tb, g->stream))) return rc;
   JGPM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp.p, tb, (int*)keep.p, (int64_t*)pos.p, m, s));
   int64_t last_pos = 0;
   int last_keep = 0;
@@ -424,15 +504,15 @@ int ensure_dag(jgpm_graph* g) {
     JGPM_CUDA_TRY(cudaStreamSynchronize(s));
   }
   const int64_t total = last_pos + last_keep;
-  if ((rc = dalloc(&g->d_dag_col, total))) return rc;
+  if ((rc = dalloc(&g->d_dag_col, total, g->stream))) return rc;
   k_orient_scatter<<<grid_for(m), 256, 0, s>>>(g->d_col, (int*)keep.p, (int64_t*)pos.p, m,
                                                g->d_dag_col);
   k_dag_rowptr<<<grid_for((int64_t)n + 1), 256, 0, s>>>(g->d_rowptr, (int64_t*)pos.p, n, m,
                                                         total, g->d_dag_rowptr);
   JGPM_CUDA_TRY(cudaGetLastError());
   g->m_dag = total;
-  DevBuf md;
-  if ((rc = dalloc((int**)&md.p, 1))) return rc;
+  DevBuf md(g->stream);
+  if ((rc = dalloc((int**)&md.p, 1, g->stream))) return rc;
   JGPM_CUDA_TRY(cudaMemsetAsync(md.p, 0, sizeof(int), s));
   k_max_degree<<<grid_for(n), 256, 0, s>>>(g->d_dag_rowptr, n, (int*)md.p);
   int h = 0;
@@ -468,34 +548,36 @@ int ensure_tiers(jgpm_graph* g, int min_deg) {
   min_deg = 2;
   if (g->tiers.d_roots && g->tiers.min_deg == min_deg) return JGPM_OK;
   if (g->tiers.d_roots) {
-    cudaFree(g->tiers.d_roots);
+    gfree(g->tiers.d_roots, g->stream);
     g->tiers.d_roots = nullptr;
   }
   cudaStream_t s = g->stream;
   const int32_t n = g->n;
-  DevBuf k0, k1, v1, tmp;
-  if ((rc = dalloc((uint32_t**)&k0.p, n))) return rc;
-  if ((rc = dalloc((uint32_t**)&k1.p, n))) return rc;
-  if ((rc = dalloc((int32_t**)&v1.p, n))) return rc;
-  if ((rc = dalloc(&g->tiers.d_roots, n))) return rc;
+  DevBuf k0(g->stream), k1(g->stream), v1(g->stream), tmp(g->stream);
+  if ((rc = dalloc((uint32_t**)&k0.p, n, g->stream))) return rc;
+  if ((rc = dalloc((uint32_t**)&k1.p, n, g->stream))) return rc;
+  if ((rc = dalloc((int32_t**)&v1.p, n, g->stream))) return rc;
+  if ((rc = dalloc(&g->tiers.d_roots, n, g->stream))) return rc;
   k_root_keys<<<grid_for(n), 256, 0, s>>>(g->d_dag_rowptr, n, min_deg, (uint32_t*)k0.p,
                                           g->tiers.d_roots);
+  // keys are out-degrees: sort only the bits the largest one needs
+  const int key_bits = std::max(1, 32 - __builtin_clz((unsigned)std::max(1, g->max_out_degree)));
   size_t tb = 0;
   JGPM_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(
-      nullptr, tb, (uint32_t*)k0.p, (uint32_t*)k1.p, g->tiers.d_roots, (int32_t*)v1.p, n, 0, 32,
-      s));
-  if ((rc = dalloc((char**)&tmp.p, tb))) return rc;
+      nullptr, tb, (uint32_t*)k0.p, (uint32_t*)k1.p, g->tiers.d_roots, (int32_t*)v1.p, n, 0,
+      key_bits, s));
+  if ((rc = dalloc((char**)&tmp.p, tb, g->stream))) return rc;
   JGPM_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(
-      tmp.p, tb, (uint32_t*)k0.p, (uint32_t*)k1.p, g->tiers.d_roots, (int32_t*)v1.p, n, 0, 32,
-      s));
+      tmp.p, tb, (uint32_t*)k0.p, (uint32_t*)k1.p, g->tiers.d_roots, (int32_t*)v1.p, n, 0,
+      key_bits, s));
   // keys descending: [>kMidMaxDeg][33..kMidMaxDeg][min_deg..32][0...].  The tier boundaries
   // (first index with key <= x for each threshold x) are found on the device; only they come
   // back to the host.
   JGPM_CUDA_TRY(cudaMemcpyAsync(g->tiers.d_roots, v1.p, (size_t)n * sizeof(int32_t),
                                 cudaMemcpyDeviceToDevice, s));
   constexpr int kNThr = 34 + 7;  // 0..33, then 64, 128, 256, 512, 1024, 2048, 4096
-  DevBuf bnd;
-  if ((rc = dalloc((int64_t**)&bnd.p, kNThr))) return rc;
+  DevBuf bnd(g->stream);
+  if ((rc = dalloc((int64_t**)&bnd.p, kNThr, g->stream))) return rc;
   k_tier_bounds<<<1, 64, 0, s>>>((const uint32_t*)k1.p, n, (int64_t*)bnd.p);
   JGPM_CUDA_TRY(cudaGetLastError());
   int64_t hb[kNThr];
@@ -519,49 +601,53 @@ int ensure_tiers(jgpm_graph* g, int min_deg) {
 int ensure_control(jgpm_graph* g) {
   if (g->d_ctl) return JGPM_OK;
   int rc;
-  if ((rc = dalloc(&g->d_ctl, 1))) return rc;
-  JGPM_CUDA_TRY(cudaMallocHost((void**)&g->h_ctl, sizeof(DevControl)));
+  if ((rc = dalloc(&g->d_ctl, 1, g->stream))) return rc;
+  g->h_ctl = ctl_slot();
+  if (!g->h_ctl) {
+    jgpm_set_error_("pinned host allocation of a control block failed");
+    return JGPM_ENOMEM;
+  }
   memset(g->h_ctl, 0, sizeof(DevControl));
   return JGPM_OK;
 }
 
 int ensure_scratch(jgpm_graph* g, size_t bytes) {
   if (g->scratch_bytes >= bytes) return JGPM_OK;
-  if (g->d_scratch) cudaFree(g->d_scratch);
+  if (g->d_scratch) gfree(g->d_scratch, g->stream);
   g->d_scratch = nullptr;
   g->scratch_bytes = 0;
   int rc;
-  if ((rc = dalloc((char**)&g->d_scratch, bytes))) return rc;
+  if ((rc = dalloc((char**)&g->d_scratch, bytes, g->stream))) return rc;
   g->scratch_bytes = bytes;
   return JGPM_OK;
 }
 
 int ensure_aux(jgpm_graph* g, size_t bytes) {
   if (g->aux_bytes >= bytes) return JGPM_OK;
-  if (g->d_aux) cudaFree(g->d_aux);
+  if (g->d_aux) gfree(g->d_aux, g->stream);
   g->d_aux = nullptr;
   g->aux_bytes = 0;
   int rc;
-  if ((rc = dalloc((char**)&g->d_aux, bytes))) return rc;
+  if ((rc = dalloc((char**)&g->d_aux, bytes, g->stream))) return rc;
   g->aux_bytes = bytes;
   return JGPM_OK;
 }
 
 void free_graph_device(jgpm_graph* g) {
-  cudaFree(g->d_rowptr);
-  cudaFree(g->d_col);
-  cudaFree(g->d_dag_rowptr);
-  cudaFree(g->d_dag_col);
-  cudaFree(g->d_rank_rowptr);
-  cudaFree(g->d_rank_col);
-  cudaFree(g->d_c4_small);
-  cudaFree(g->d_c4_mid);
-  cudaFree(g->d_c4_large);
-  cudaFree(g->tiers.d_roots);
-  cudaFree(g->d_ctl);
-  cudaFree(g->d_scratch);
-  cudaFree(g->d_aux);
-  if (g->h_ctl) cudaFreeHost(g->h_ctl);
+  gfree(g->d_rowptr, g->stream);
+  gfree(g->d_col, g->stream);
+  gfree(g->d_dag_rowptr, g->stream);
+  gfree(g->d_dag_col, g->stream);
+  gfree(g->d_rank_rowptr, g->stream);
+  gfree(g->d_rank_col, g->stream);
+  gfree(g->d_c4_small, g->stream);
+  gfree(g->d_c4_mid, g->stream);
+  gfree(g->d_c4_large, g->stream);
+  gfree(g->tiers.d_roots, g->stream);
+  gfree(g->d_ctl, g->stream);
+  gfree(g->d_scratch, g->stream);
+  gfree(g->d_aux, g->stream);
+  ctl_release(g->h_ctl);
   if (g->stream) cudaStreamDestroy(g->stream);
 }
 
@@ -610,36 +696,36 @@ int ensure_rank_csr(jgpm_graph* g) {
   const int64_t m = g->m;
   const int shift = shift_for(n);
   int rc;
-  DevBuf k0, k1, v0, v1, rank, src, tmp;
-  if ((rc = dalloc((uint64_t**)&k0.p, n))) return rc;
-  if ((rc = dalloc((uint64_t**)&k1.p, n))) return rc;
-  if ((rc = dalloc((int32_t**)&v0.p, n))) return rc;
-  if ((rc = dalloc((int32_t**)&v1.p, n))) return rc;
-  if ((rc = dalloc((int32_t**)&rank.p, n))) return rc;
+  DevBuf k0(g->stream), k1(g->stream), v0(g->stream), v1(g->stream), rank(g->stream), src(g->stream), tmp(g->stream);
+  if ((rc = dalloc((uint64_t**)&k0.p, n, g->stream))) return rc;
+  if ((rc = dalloc((uint64_t**)&k1.p, n, g->stream))) return rc;
+  if ((rc = dalloc((int32_t**)&v0.p, n, g->stream))) return rc;
+  if ((rc = dalloc((int32_t**)&v1.p, n, g->stream))) return rc;
+  if ((rc = dalloc((int32_t**)&rank.p, n, g->stream))) return rc;
   k_rank_keys<<<grid_for(n), 256, 0, s>>>(g->d_rowptr, n, (uint64_t*)k0.p, (int32_t*)v0.p);
   size_t tb = 0;
   JGPM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t*)k0.p, (uint64_t*)k1.p,
                                                 (int32_t*)v0.p, (int32_t*)v1.p, n, 0, 64, s));
-  if ((rc = dalloc((char**)&tmp.p, tb))) return rc;
+  if ((rc = dalloc((char**)&tmp.p, tb, g->stream))) return rc;
   JGPM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp.p, tb, (uint64_t*)k0.p, (uint64_t*)k1.p,
                                                 (int32_t*)v0.p, (int32_t*)v1.p, n, 0, 64, s));
   k_invert<<<grid_for(n), 256, 0, s>>>((int32_t*)v1.p, n, (int32_t*)rank.p);
   // arcs as (rank(u), rank(v)) keys, sorted
-  DevBuf ak, ak2, tmp2;
-  if ((rc = dalloc((int32_t**)&src.p, m))) return rc;
-  if ((rc = dalloc((uint64_t**)&ak.p, m))) return rc;
-  if ((rc = dalloc((uint64_t**)&ak2.p, m))) return rc;
+  DevBuf ak(g->stream), ak2(g->stream), tmp2(g->stream);
+  if ((rc = dalloc((int32_t**)&src.p, m, g->stream))) return rc;
+  if ((rc = dalloc((uint64_t**)&ak.p, m, g->stream))) return rc;
+  if ((rc = dalloc((uint64_t**)&ak2.p, m, g->stream))) return rc;
   k_arc_src<<<grid_for((int64_t)n * 32), 256, 0, s>>>(g->d_rowptr, n, (int32_t*)src.p);
   k_rank_arc_keys<<<grid_for(m), 256, 0, s>>>((int32_t*)src.p, g->d_col, (int32_t*)rank.p, m,
                                               shift, (uint64_t*)ak.p);
   cub::DoubleBuffer<uint64_t> db((uint64_t*)ak.p, (uint64_t*)ak2.p);
   size_t tb2 = 0;
   JGPM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tb2, db, m, 0, 2 * shift, s));
-  if ((rc = dalloc((char**)&tmp2.p, tb2))) return rc;
+  if ((rc = dalloc((char**)&tmp2.p, tb2, g->stream))) return rc;
   JGPM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(tmp2.p, tb2, db, m, 0, 2 * shift, s));
-  if ((rc = dalloc(&g->d_rank_rowptr, (size_t)n + 1))) return rc;
-  if ((rc = dalloc(&g->d_rank_col, m))) {
-    cudaFree(g->d_rank_rowptr);
+  if ((rc = dalloc(&g->d_rank_rowptr, (size_t)n + 1, g->stream))) return rc;
+  if ((rc = dalloc(&g->d_rank_col, m, g->stream))) {
+    gfree(g->d_rank_rowptr, g->stream);
     g->d_rank_rowptr = nullptr;
     return rc;
   }
@@ -728,18 +814,18 @@ int evict_graph(jgpm_graph* g, std::vector<int64_t>& h_rowptr, std::vector<int32
                                     cudaMemcpyDeviceToHost, g->stream));
   }
   JGPM_CUDA_TRY(cudaStreamSynchronize(g->stream));
-  cudaFree(g->d_rowptr);
-  cudaFree(g->d_col);
-  cudaFree(g->d_dag_rowptr);
-  cudaFree(g->d_dag_col);
-  cudaFree(g->d_rank_rowptr);
-  cudaFree(g->d_rank_col);
-  cudaFree(g->d_c4_small);
-  cudaFree(g->d_c4_mid);
-  cudaFree(g->d_c4_large);
-  cudaFree(g->tiers.d_roots);
-  cudaFree(g->d_scratch);
-  cudaFree(g->d_aux);
+  gfree(g->d_rowptr, g->stream);
+  gfree(g->d_col, g->stream);
+  gfree(g->d_dag_rowptr, g->stream);
+  gfree(g->d_dag_col, g->stream);
+  gfree(g->d_rank_rowptr, g->stream);
+  gfree(g->d_rank_col, g->stream);
+  gfree(g->d_c4_small, g->stream);
+  gfree(g->d_c4_mid, g->stream);
+  gfree(g->d_c4_large, g->stream);
+  gfree(g->tiers.d_roots, g->stream);
+  gfree(g->d_scratch, g->stream);
+  gfree(g->d_aux, g->stream);
   g->d_aux = nullptr;
   g->aux_bytes = 0;
   g->d_rank_rowptr = nullptr;

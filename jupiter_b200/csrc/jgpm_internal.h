@@ -116,6 +116,11 @@ void jgpm_set_error_(const std::string& msg);
 
 namespace jgpm {
 // graph_build.cu
+// Device memory of graphs and their temporaries: a per-device stream-ordered pool that keeps
+// freed memory for reuse (freed memory is reused in the order of the freeing stream), so a
+// graph's life cycle does not pay cudaMalloc / cudaFree.  gfree(nullptr) does nothing.
+int gmalloc(void** p, size_t bytes, cudaStream_t s);
+void gfree(void* p, cudaStream_t s);
 int build_from_edges_device(jgpm_graph* g, int32_t n, int64_t* d_keys, int64_t nkeys_valid_cap);
 int rmat_build(jgpm_graph* g, int64_t n, int64_t num_edges, double a, double b, double c,
                uint64_t seed);
