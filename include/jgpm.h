@@ -192,6 +192,19 @@ int jgpm_count_shard(jgpm_graph* g, const char* pattern, int induced, int32_t sh
  * begins, and do not reset the device (cudaDeviceReset) between calls. */
 int jgpm_count_noalloc(jgpm_graph* g, const char* pattern, int induced, uint64_t* out);
 
+/* Listing mode: writes the embeddings themselves, k vertex ids each (k = the pattern's size),
+ * to out[0 .. k * min(total, capacity)) and their number to *total (all of them, also when
+ * more than capacity exist: call with capacity 0 to size the buffer).  out may be host or
+ * device memory.  Patterns: "triangle" and the k-cliques up to k = 8 (vertices in DAG order),
+ * "4-cycle"/"P1" (cycle order v0 - v1 - v3 - v2 from the largest vertex v0, v1 > v2) and
+ * "diamond"/"P2" (the shared edge v0 > v1, then the other two, ascending) with induced = 0;
+ * "4-cycle", "diamond", "tailed-triangle", "4-path", "3-star" with induced = 1 (the root arc's
+ * two vertices, then the other two).  The order of the tuples is unspecified.  The
+ * reference chooses counting or listing when it is built (common.mk:60-63) and only counts;
+ * this is the listing counterpart of jgpm_count's plans. */
+int jgpm_list(jgpm_graph* g, const char* pattern, int induced, int32_t* out, int64_t capacity,
+              int64_t* total, jgpm_stats* st);
+
 /* Vertex-induced census of the six connected 4-vertex graphlets, out[0..5] = 3-star,
  * 4-path, tailed triangle, 4-cycle, diamond, 4-clique. */
 int jgpm_census4(jgpm_graph* g, uint64_t out[6], jgpm_stats* st);

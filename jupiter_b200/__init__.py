@@ -145,6 +145,8 @@ def lib():
                                    ctypes.c_int64, ctypes.c_int64, _PU64, ctypes.POINTER(_Stats)]
     L.jgpm_count_shard.argtypes = [G, ctypes.c_char_p, ctypes.c_int, ctypes.c_int32,
                                    ctypes.c_int32, _PU64, ctypes.POINTER(_Stats)]
+    L.jgpm_list.argtypes = [G, ctypes.c_char_p, ctypes.c_int, _P32, ctypes.c_int64,
+                            _P64, ctypes.POINTER(_Stats)]
     L.jgpm_census4.argtypes = [G, _PU64, ctypes.POINTER(_Stats)]
     L.jgpm_setop.argtypes = [ctypes.c_int, _P32, ctypes.c_int32, _P32, ctypes.c_int32,
                              ctypes.c_int32, ctypes.c_int32, _P32, _P32]
@@ -311,6 +313,27 @@ class Graph:
             return out.value, {"kernel_ms": st.kernel_ms, "launches": st.launches,
                                "method": METHODS.get(st.method, st.method)}
         return out.value
+
+    def list(self, pattern, induced=False, capacity=None):
+        """The embeddings of `pattern` as an (n, k) int32 array (listing mode).  capacity =
+        None sizes the buffer with a first counting pass."""
+        total = ctypes.c_int64()
+        st = _Stats()
+        if capacity is None:
+            _check(lib().jgpm_list(self._h, pattern.encode(), int(bool(induced)), None, 0,
+                                   ctypes.byref(total), ctypes.byref(st)))
+            capacity = total.value
+        k = 4
+        if not induced:
+            k = {"triangle": 3, "P0": 3, "3-clique": 3, "4-clique": 4, "P13": 4,
+                 "5-clique": 5, "P14": 5, "6-clique": 6, "P15": 6, "7-clique": 7,
+                 "P16": 7}.get(pattern, 4)
+            if pattern.startswith("k-clique:"):
+                k = int(pattern.split(":")[1])
+        out = np.zeros((max(capacity, 1), k), dtype=np.int32)
+        _check(lib().jgpm_list(self._h, pattern.encode(), int(bool(induced)), _p32(out),
+                               int(capacity), ctypes.byref(total), ctypes.byref(st)))
+        return out[: min(total.value, capacity)], total.value
 
     def census4(self):
         """Vertex-induced counts [3-star, 4-path, tailed triangle, 4-cycle, diamond, K4]."""
