@@ -25,6 +25,7 @@ set-intersection and graph loader, compiled from its sources into oracle/_ref/) 
 same plans on all host cores, over a bounded sample of root arcs of the same workload.
 """
 import argparse
+import atexit
 import json
 import os
 import statistics
@@ -71,12 +72,19 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            atexit.register(self.__exit__, None, None, None)  # never outlives the bench
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once the sampler is running: samples taken before that
+            # (nvidia-smi's start-up) are not counted
+            t_end = time.perf_counter() + 5.0
+            while not self.lines and time.perf_counter() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.first = len(self.lines)
         return self
 
     def _read(self):
@@ -84,7 +92,7 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
-        if self.proc:
+        if self.proc and self.proc.poll() is None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -94,7 +102,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.first:] or self.lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -218,10 +226,11 @@ def run_jgpm(args):
         dist.barrier()
     torch.cuda.synchronize()
     events = []
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            step(events)
-        torch.cuda.synchronize()
+    # clocks are sampled over both timed regions: the device-timed steps and the e2e steps
+    clk = ClockSampler(local).__enter__()
+    for _ in range(args.steps):
+        step(events)
+    torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -276,6 +285,7 @@ def run_jgpm(args):
         e2e_step()
         torch.cuda.synchronize()
         e2e_times.append((time.perf_counter() - t0) * 1e3)
+    clk.__exit__(None, None, None)
     e2e_ms = statistics.median(e2e_times)
     if world > 1:
         e2e_ms = shards.max_over_ranks(e2e_ms, dev)

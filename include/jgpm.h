@@ -299,7 +299,11 @@ int jgpm_server_add_graph(jgpm_server* s, jgpm_graph* g, int32_t* graph_id);
  * lane (one jgpm_count at a time, concurrently with the batches); the prefix "induced:"
  * (e.g. "induced:tailed-triangle") asks for the vertex-induced count.
  * A query is admitted to the device when its graph is resident and its estimated frontier
- * memory fits the budget; JGPM_EADMISSION if it can never fit. */
+ * memory fits the budget; JGPM_EADMISSION if it can never fit.  Pending queries are admitted
+ * shortest estimated work first, with aging: the estimate is the running average of the
+ * service times measured for the same (graph, pattern) (before the first, a prior from the
+ * graph's DAG arcs and the pattern), less 0.1 s per second the query has waited, so light
+ * queries do not wait behind heavy ones and no query waits for ever. */
 int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, uint64_t* ticket);
 
 /* Waits up to timeout_ms (< 0: no limit) for a ticket; JGPM_ETIMEDOUT if it is not done. */

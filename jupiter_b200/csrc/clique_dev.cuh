@@ -67,6 +67,42 @@ constexpr int kStage = 256;
 // of the hits of 32 entries is one word of the row (ORed into Ri, which starts at zero).
 // on_hit(j, e) runs for every hit in the edge-triangle modes (j = list index, e = the slot
 // of L[j] in the row).
+// One staged piece of a row (cl elements in stage[], the first at slot e0 of col) searched
+// for the root's list: each lane binary-searches two list entries, and the ballot of the hits
+// of 32 entries is one word of the row.
+template <bool ETRI, typename F>
+__device__ __forceinline__ void flip_search(const vid_t* stage, int cl, eid_t e0, const vid_t* L,
+                                            int d, int w_d, uint32_t* Ri, F&& on_hit) {
+  const int lane = threadIdx.x & 31;
+  const int top = top_pow2(cl);
+  for (int q0 = 0; q0 < w_d; q0 += 2) {
+    const int ja = 32 * q0 + lane, jb = ja + 32;
+    const vid_t xa = ja < d ? L[ja] : INT32_MAX;
+    const vid_t xb = jb < d ? L[jb] : INT32_MAX;
+    int pa, pb;
+    count_below2(stage, cl, top, xa, xb, pa, pb);
+    const bool fa = ja < d && pa < cl && stage[pa] == xa;
+    const bool fb = jb < d && pb < cl && stage[pb] == xb;
+    const unsigned ma = __ballot_sync(kFull, fa), mb = __ballot_sync(kFull, fb);
+    if (lane == 0) {
+      if (ma) atomicOr(Ri + q0, ma);
+      if (mb && q0 + 1 < w_d) atomicOr(Ri + q0 + 1, mb);
+    }
+    if (ETRI) {
+      if (fa) on_hit(ja, e0 + pa);
+      if (fb) on_hit(jb, e0 + pb);
+    }
+  }
+}
+
+// Row i of a root's bitmap when the row (len elements from col + rsi, sorted) is longer than
+// the root's list L[0..d): the list is looked up in the row, as the reference does with the
+// shorter of two lists.  Used by the warp tier, whose lists (out-degree <= 128) are mostly
+// shorter than their rows; in the CTA bands the extra registers cost more than they save.  A
+// warp stages up to kStage row elements at a time in shared memory (one coalesced copy) and
+// searches them (flip_search); the hits are ORed into Ri, which starts at zero.  on_hit(j, e)
+// runs for every hit in the edge-triangle modes (j = list index, e = the slot of L[j] in the
+// row).
 template <bool ETRI, typename F>
 __device__ __forceinline__ void flip_row(const vid_t* __restrict__ col, eid_t rsi, int len,
                                          const vid_t* L, int d, int w_d, uint32_t* Ri,
@@ -77,25 +113,7 @@ __device__ __forceinline__ void flip_row(const vid_t* __restrict__ col, eid_t rs
     __syncwarp();
     for (int t = lane; t < cl; t += 32) stage[t] = __ldg(col + rsi + c0 + t);
     __syncwarp();
-    const int top = top_pow2(cl);
-    for (int q0 = 0; q0 < w_d; q0 += 2) {
-      const int ja = 32 * q0 + lane, jb = ja + 32;
-      const vid_t xa = ja < d ? L[ja] : INT32_MAX;
-      const vid_t xb = jb < d ? L[jb] : INT32_MAX;
-      int pa, pb;
-      count_below2(stage, cl, top, xa, xb, pa, pb);
-      const bool fa = ja < d && pa < cl && stage[pa] == xa;
-      const bool fb = jb < d && pb < cl && stage[pb] == xb;
-      const unsigned ma = __ballot_sync(kFull, fa), mb = __ballot_sync(kFull, fb);
-      if (lane == 0) {
-        if (ma) atomicOr(Ri + q0, ma);
-        if (mb && q0 + 1 < w_d) atomicOr(Ri + q0 + 1, mb);
-      }
-      if (ETRI) {
-        if (fa) on_hit(ja, rsi + c0 + pa);
-        if (fb) on_hit(jb, rsi + c0 + pb);
-      }
-    }
+    flip_search<ETRI>(stage, cl, rsi + c0, L, d, w_d, Ri, on_hit);
   }
   __syncwarp();
 }
@@ -367,7 +385,11 @@ struct WarpSmem {
   vid_t stage[kStage];      // a long row, staged to look the root's list up in it
 };
 
-template <int K, bool STATS, bool ETRI, bool PAIRS = false, bool TT = false>
+// PIPE: the rows that are looked up in (flip rows) go through a register pipeline: while a
+// warp searches one staged piece, the next piece (of this row or of the next flip row) is
+// already on its way into registers, so the row loads no longer stall the searches.  It costs
+// kStage / 32 registers per lane, which pays in the plain k <= 4 warp tier only.
+template <int K, bool STATS, bool ETRI, bool PAIRS = false, bool TT = false, bool PIPE = false>
 __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
                                            const vid_t* __restrict__ col, vid_t u, WarpSmem& ws,
                                            uint32_t* tri, acc_t& elems,
@@ -434,6 +456,51 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
       }
     }
   };
+  auto etri_hit = [&](int j, eid_t e) {
+    const unsigned o = atomicAdd(tri + e, 1u);
+    if (PAIRS) pairs += (acc_t)o;
+    atomicAdd(&ws.colcnt[j], 1);
+  };
+  if (PIPE && !STATS) {
+    constexpr int kPer = kStage / 32;
+    auto next_flip = [&](int r) {
+      for (++r; r < d; ++r) {
+        const int l = ws.deg[r];
+        if (l >= kLongRow && l > d) break;
+      }
+      return r;
+    };
+    vid_t nb[kPer];
+    auto fetch = [&](int r, int c) {
+      const eid_t s = ws.rs[r] + c;
+      const int n = min(kStage, ws.deg[r] - c);
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) {
+        const int t = q * 32 + lane;
+        nb[q] = t < n ? __ldg(col + s + t) : 0;
+      }
+    };
+    int i = next_flip(-1), c0 = 0;
+    if (i < d) fetch(i, 0);
+    while (i < d) {
+      const int cl = min(kStage, ws.deg[i] - c0);
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < kPer; ++q)
+        if (q * 32 + lane < cl) ws.stage[q * 32 + lane] = nb[q];
+      __syncwarp();
+      int ni = i, nc = c0 + kStage;
+      if (nc >= ws.deg[i]) {
+        ni = next_flip(i);
+        nc = 0;
+      }
+      if (ni < d) fetch(ni, nc);
+      flip_search<ETRI>(ws.stage, cl, ws.rs[i] + c0, ws.L, d, w_d, ws.R + i * w_d, etri_hit);
+      i = ni;
+      c0 = nc;
+    }
+    __syncwarp();
+  }
   // long rows: the warp scans one row at a time, two elements per lane and iteration, so no
   // element searches for its row
   if (!STATS) {
@@ -442,12 +509,8 @@ __device__ __forceinline__ acc_t warp_root(const eid_t* __restrict__ rowptr,
       if (len < kLongRow) continue;
       const eid_t rsi = ws.rs[i];
       if (len > d) {  // the row is the longer list: look the root's list up in it
-        flip_row<ETRI>(col, rsi, len, ws.L, d, w_d, ws.R + i * w_d, ws.stage,
-                       [&](int j, eid_t e) {
-                         const unsigned o = atomicAdd(tri + e, 1u);
-                         if (PAIRS) pairs += (acc_t)o;
-                         atomicAdd(&ws.colcnt[j], 1);
-                       });
+        if (PIPE) continue;
+        flip_row<ETRI>(col, rsi, len, ws.L, d, w_d, ws.R + i * w_d, ws.stage, etri_hit);
         continue;
       }
       for (int t0 = lane; t0 < len; t0 += 64) {

@@ -126,8 +126,8 @@ __global__ void __launch_bounds__(256, 4) k_clique_warp(CliqueArgs a) {
     c0 = __shfl_sync(kFull, c0, 0);
     const int64_t idx = a.begin + (int64_t)c0;
     if (idx >= a.end) break;
-    cnt += warp_root<K, STATS, ETRI, PAIRS, TT>(a.rowptr, a.col, root_at(a, idx), ws, a.tri, elems,
-                                                 a.srow);
+    cnt += warp_root<K, STATS, ETRI, PAIRS, TT, (K <= 4)>(a.rowptr, a.col, root_at(a, idx), ws,
+                                                           a.tri, elems, a.srow);
   }
   for (int o = 16; o > 0; o >>= 1) {
     cnt += __shfl_xor_sync(kFull, cnt, o);
