@@ -350,6 +350,31 @@ int jgpm_setop_batch(int op, const int32_t* a, const int64_t* a_off, const int32
                      const int32_t* exclude, int32_t* counts, int32_t* out,
                      const int64_t* out_off);
 
+/* Fused splits: one call yields several of the sets above at once.
+ *   JGPM_SPLIT_FUSE     c = A \ B, d = A & B, e = B \ A;  count = |A & B|
+ *                       (fuse_set, include/set_difference.cuh:248-343)
+ *   JGPM_SPLIT_DIF_INT  c = {x in A : x < upper, x not in B}, d = the rest of A (members of B
+ *                       and keys at or above upper);  count = |c|
+ *                       (dif_int_set, include/set_difference.cuh:346-413; with upper =
+ *                       INT32_MAX the unbounded form, :415-475)
+ * Every output is in ascending order; |c| and |d| follow from count and na (and |e| from nb).
+ * Capacities: c and d na entries, e nb entries (e is unused by JGPM_SPLIT_DIF_INT and may be
+ * NULL); upper is ignored by JGPM_SPLIT_FUSE.  Outputs the sizes leave unwritten keep their
+ * contents.  Note: the reference's templates return 0 and write nothing when A or B is empty;
+ * these entry points follow the set algebra there too (B empty: c = A below upper). */
+#define JGPM_SPLIT_FUSE 0
+#define JGPM_SPLIT_DIF_INT 1
+int jgpm_setop_split(int kind, const int32_t* a, int32_t na, const int32_t* b, int32_t nb,
+                     int32_t upper, int32_t* c, int32_t* d, int32_t* e, int32_t* count);
+
+/* A batch of fused splits in one launch (one warp per pair), pairs given by offsets as in
+ * jgpm_setop_batch.  Pair i writes c[a_off[i] ..) and d[a_off[i] ..) (arrays of a_off[nops]
+ * entries) and e[b_off[i] ..) (b_off[nops] entries): the outputs are laid out like the
+ * inputs.  upper may be NULL (no bounds).  Host or device arrays. */
+int jgpm_setop_split_batch(int kind, const int32_t* a, const int64_t* a_off, const int32_t* b,
+                           const int64_t* b_off, int64_t nops, const int32_t* upper,
+                           int32_t* counts, int32_t* c, int32_t* d, int32_t* e);
+
 #ifdef __cplusplus
 }
 #endif

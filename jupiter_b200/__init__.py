@@ -9,6 +9,8 @@ reference's operator surface:
                                        count reduction (src/jupiter_gpm.cu:356-908)
 * ``setop(...)`` / ``setop_batch``  -- the intersect / difference templates
                                        (include/set_intersect.cuh, include/set_difference.cuh)
+* ``setop_split(...)``              -- the fused splits fuse_set / dif_int_set
+                                       (include/set_difference.cuh:248-475)
 * ``solve(prefix, pattern, rounds)`` -- the CLI `jupiter_gpm <graph> <pattern> [rounds]`
                                        (src/main.cc:7-47), printing the same result line.
 
@@ -22,8 +24,10 @@ import time
 import numpy as np
 
 __all__ = [
-    "JgpmError", "Graph", "setop", "setop_batch", "solve", "lib", "library_path",
+    "JgpmError", "Graph", "setop", "setop_batch", "setop_split", "setop_split_batch",
+    "solve", "lib", "library_path",
     "OP_INTERSECT", "OP_INTERSECT_COUNT", "OP_DIFFERENCE", "OP_DIFFERENCE_COUNT",
+    "SPLIT_FUSE", "SPLIT_DIF_INT",
     "COUNT_STATS", "COUNT_FORCE_PLAN", "COUNT_FORCE_ENUM", "STATUS", "batch_count",
     "autotune", "Tuning", "Server",
 ]
@@ -31,6 +35,7 @@ __all__ = [
 _PKG = os.path.dirname(os.path.abspath(__file__))
 
 OP_INTERSECT, OP_INTERSECT_COUNT, OP_DIFFERENCE, OP_DIFFERENCE_COUNT = 0, 1, 2, 3
+SPLIT_FUSE, SPLIT_DIF_INT = 0, 1
 COUNT_STATS, COUNT_FORCE_PLAN, COUNT_FORCE_ENUM = 1, 2, 4
 
 STATUS = {
@@ -152,6 +157,10 @@ def lib():
                              ctypes.c_int32, ctypes.c_int32, _P32, _P32]
     L.jgpm_setop_batch.argtypes = [ctypes.c_int, _P32, _P64, _P32, _P64, ctypes.c_int64, _P32,
                                    _P32, _P32, _P32, _P64]
+    L.jgpm_setop_split.argtypes = [ctypes.c_int, _P32, ctypes.c_int32, _P32, ctypes.c_int32,
+                                   ctypes.c_int32, _P32, _P32, _P32, _P32]
+    L.jgpm_setop_split_batch.argtypes = [ctypes.c_int, _P32, _P64, _P32, _P64, ctypes.c_int64,
+                                         _P32, _P32, _P32, _P32, _P32]
     L.jgpm_batch_count.argtypes = [ctypes.POINTER(_Job), ctypes.c_int32, ctypes.POINTER(Tuning),
                                    _PU64, ctypes.POINTER(_BatchStats)]
     V = ctypes.c_void_p
@@ -511,6 +520,57 @@ def setop_batch(op, a_lists, b_lists, upper=None, exclude=None):
     if mat:
         return counts, [out[out_off[i]: out_off[i] + counts[i]].copy() for i in range(nops)]
     return counts
+
+
+def _split_lists(kind, a, b, r):
+    """(c, d, e) of one pair from its count (e None for SPLIT_DIF_INT)."""
+    if kind == SPLIT_FUSE:
+        return (len(a) - r, r, len(b) - r)
+    return (r, len(a) - r, None)
+
+
+def setop_split(kind, a, b, upper=None):
+    """One fused split (SPLIT_FUSE: A \\ B, A & B, B \\ A; SPLIT_DIF_INT: A below upper
+    minus B, and the rest of A); returns (count, c, d, e), e None for SPLIT_DIF_INT."""
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    b = np.ascontiguousarray(b, dtype=np.int32)
+    up = np.iinfo(np.int32).max if upper is None else int(upper)
+    c = np.empty(max(len(a), 1), np.int32)
+    d = np.empty(max(len(a), 1), np.int32)
+    e = np.empty(max(len(b), 1), np.int32)
+    n = ctypes.c_int32()
+    _check(lib().jgpm_setop_split(kind, _p32(a), len(a), _p32(b), len(b), up, _p32(c), _p32(d),
+                                  _p32(e) if kind == SPLIT_FUSE else None, ctypes.byref(n)))
+    nc, nd, ne = _split_lists(kind, a, b, n.value)
+    return n.value, c[:nc].copy(), d[:nd].copy(), (e[:ne].copy() if ne is not None else None)
+
+
+def setop_split_batch(kind, a_lists, b_lists, upper=None):
+    """Many fused splits in one launch; returns the counts and, per pair, (c, d, e)."""
+    nops = len(a_lists)
+    a_off = np.zeros(nops + 1, dtype=np.int64)
+    b_off = np.zeros(nops + 1, dtype=np.int64)
+    a_off[1:] = np.cumsum([len(x) for x in a_lists])
+    b_off[1:] = np.cumsum([len(x) for x in b_lists])
+    a = np.concatenate([np.asarray(x, dtype=np.int32) for x in a_lists] + [np.zeros(0, np.int32)])
+    b = np.concatenate([np.asarray(x, dtype=np.int32) for x in b_lists] + [np.zeros(0, np.int32)])
+    counts = np.zeros(max(nops, 1), dtype=np.int32)
+    c = np.empty(max(len(a), 1), np.int32)
+    d = np.empty(max(len(a), 1), np.int32)
+    e = np.empty(max(len(b), 1), np.int32)
+    up = None if upper is None else np.ascontiguousarray(upper, dtype=np.int32)
+    _check(lib().jgpm_setop_split_batch(kind, _p32(a), _p64(a_off), _p32(b), _p64(b_off), nops,
+                                        _p32(up) if up is not None else None, _p32(counts),
+                                        _p32(c), _p32(d),
+                                        _p32(e) if kind == SPLIT_FUSE else None))
+    counts = counts[:nops]
+    out = []
+    for i in range(nops):
+        nc, nd, ne = _split_lists(kind, a_lists[i], b_lists[i], int(counts[i]))
+        a0, b0 = int(a_off[i]), int(b_off[i])
+        out.append((c[a0: a0 + nc].copy(), d[a0: a0 + nd].copy(),
+                    e[b0: b0 + ne].copy() if ne is not None else None))
+    return counts, out
 
 
 def solve(prefix, pattern, rounds=1, print_result=True):

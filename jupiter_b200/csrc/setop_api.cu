@@ -44,6 +44,30 @@ __global__ void k_setop_batch(int op, const int32_t* a, const int64_t* a_off, co
   }
 }
 
+// Fused splits, one warp per pair; pair i's outputs sit at the offsets of its operands
+// (c and d at a_off[i], e at b_off[i]).
+__global__ void k_split_batch(int kind, const int32_t* a, const int64_t* a_off, const int32_t* b,
+                              const int64_t* b_off, int64_t nops, const int32_t* upper,
+                              int32_t* counts, int32_t* c, int32_t* d, int32_t* e) {
+  const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nops;
+       i += warps) {
+    const int64_t a0 = a_off[i], b0 = b_off[i];
+    const int32_t* A = a + a0;
+    const int na = (int)(a_off[i + 1] - a0);
+    const int32_t* B = b + b0;
+    const int nb = (int)(b_off[i + 1] - b0);
+    int r;
+    if (kind == JGPM_SPLIT_FUSE) {
+      r = na - warp_split_by(A, na, B, nb, INT32_MAX, c + a0, d + a0);  // |A & B|
+      warp_split_by(B, nb, A, na, INT32_MAX, e + b0, nullptr);
+    } else {
+      r = warp_split_by(A, na, B, nb, upper ? upper[i] : INT32_MAX, c + a0, d + a0);
+    }
+    if ((threadIdx.x & 31) == 0) counts[i] = r;
+  }
+}
+
 bool is_device_ptr(const void* p) {
   if (!p) return false;
   cudaPointerAttributes attr;
@@ -73,6 +97,37 @@ struct Staged {
   }
   ~Staged() {
     if (owned && d) cudaFree(d);
+  }
+};
+
+// A caller's output array on the device: used in place when it is device memory, else a
+// device copy of its current contents (so entries the kernel does not write keep their
+// values either way) that back() returns to the caller.
+struct OutArray {
+  int32_t* user = nullptr;
+  int32_t* d = nullptr;
+  size_t n = 0;
+  bool staged = false;
+  cudaError_t init(int32_t* p, size_t count, cudaStream_t s) {
+    user = p;
+    n = count;
+    if (!p) return cudaSuccess;
+    if (is_device_ptr(p)) {
+      d = p;
+      return cudaSuccess;
+    }
+    staged = true;
+    cudaError_t e = cudaMalloc((void**)&d, std::max<size_t>(count, 1) * sizeof(int32_t));
+    if (e != cudaSuccess) return e;
+    if (count) return cudaMemcpyAsync(d, p, count * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    return cudaSuccess;
+  }
+  cudaError_t back(cudaStream_t s) {
+    if (!staged || !n) return cudaSuccess;
+    return cudaMemcpyAsync(user, d, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  }
+  ~OutArray() {
+    if (staged && d) cudaFree(d);
   }
 };
 
@@ -178,6 +233,88 @@ int jgpm_setop_batch(int op, const int32_t* a, const int64_t* a_off, const int32
     jgpm_set_error_(std::string("jgpm_setop_batch: ") + cudaGetErrorString(e));
     return JGPM_ECUDA;
   }
+  return JGPM_OK;
+}
+
+int jgpm_setop_split_batch(int kind, const int32_t* a, const int64_t* a_off, const int32_t* b,
+                           const int64_t* b_off, int64_t nops, const int32_t* upper,
+                           int32_t* counts, int32_t* c, int32_t* d, int32_t* e) {
+  const bool fuse = kind == JGPM_SPLIT_FUSE;
+  if ((!fuse && kind != JGPM_SPLIT_DIF_INT) || nops < 0 || !a_off || !b_off || !counts) {
+    jgpm_set_error_("jgpm_setop_split_batch: bad arguments");
+    return JGPM_EINVAL;
+  }
+  if (nops == 0) return JGPM_OK;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    jgpm_set_error_("no CUDA device");
+    return JGPM_ENODEV;
+  }
+  std::vector<int64_t> ha(nops + 1), hb(nops + 1);
+  JGPM_CUDA_TRY(cudaMemcpy(ha.data(), a_off, (nops + 1) * 8, cudaMemcpyDefault));
+  JGPM_CUDA_TRY(cudaMemcpy(hb.data(), b_off, (nops + 1) * 8, cudaMemcpyDefault));
+  if (ha[0] < 0 || hb[0] < 0) {
+    jgpm_set_error_("jgpm_setop_split_batch: bad offsets");
+    return JGPM_EINVAL;
+  }
+  if ((ha[nops] > 0 && (!c || !d)) || (fuse && hb[nops] > 0 && !e)) {
+    jgpm_set_error_("jgpm_setop_split_batch: missing output array");
+    return JGPM_EINVAL;
+  }
+  for (int64_t i = 0; i < nops; ++i) {
+    const int64_t na = ha[i + 1] - ha[i], nb = hb[i + 1] - hb[i];
+    if (na < 0 || nb < 0 || na > INT32_MAX || nb > INT32_MAX) {
+      jgpm_set_error_("jgpm_setop_split_batch: bad offsets");
+      return JGPM_EINVAL;
+    }
+  }
+  cudaStream_t s = nullptr;
+  JGPM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } sg{s};
+  Staged<int32_t> da, db, dup;
+  Staged<int64_t> dao, dbo;
+  JGPM_CUDA_TRY(da.init(a, (size_t)ha[nops], s));
+  JGPM_CUDA_TRY(db.init(b, (size_t)hb[nops], s));
+  JGPM_CUDA_TRY(dao.init(a_off, (size_t)nops + 1, s));
+  JGPM_CUDA_TRY(dbo.init(b_off, (size_t)nops + 1, s));
+  if (!fuse) JGPM_CUDA_TRY(dup.init(upper, (size_t)nops, s));
+  OutArray oc, od, oe, on;
+  JGPM_CUDA_TRY(oc.init(c, (size_t)ha[nops], s));
+  JGPM_CUDA_TRY(od.init(d, (size_t)ha[nops], s));
+  if (fuse) JGPM_CUDA_TRY(oe.init(e, (size_t)hb[nops], s));
+  JGPM_CUDA_TRY(on.init(counts, (size_t)nops, s));
+  const int64_t blocks = std::min<int64_t>((nops + 7) / 8, 148 * 16);
+  k_split_batch<<<(int)std::max<int64_t>(1, blocks), 256, 0, s>>>(
+      kind, da.d, dao.d, db.d, dbo.d, nops, dup.d, on.d, oc.d, od.d, oe.d);
+  cudaError_t err = cudaGetLastError();
+  if (err == cudaSuccess) err = on.back(s);
+  if (err == cudaSuccess) err = oc.back(s);
+  if (err == cudaSuccess) err = od.back(s);
+  if (err == cudaSuccess) err = oe.back(s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) {
+    jgpm_set_error_(std::string("jgpm_setop_split_batch: ") + cudaGetErrorString(err));
+    return JGPM_ECUDA;
+  }
+  return JGPM_OK;
+}
+
+int jgpm_setop_split(int kind, const int32_t* a, int32_t na, const int32_t* b, int32_t nb,
+                     int32_t upper, int32_t* c, int32_t* d, int32_t* e, int32_t* count) {
+  if (na < 0 || nb < 0 || !count || (na > 0 && !a) || (nb > 0 && !b)) {
+    jgpm_set_error_("jgpm_setop_split: bad arguments");
+    return JGPM_EINVAL;
+  }
+  const int64_t aoff[2] = {0, na}, boff[2] = {0, nb};
+  const int32_t up[1] = {upper};
+  int32_t cnt = 0;
+  const int rc = jgpm_setop_split_batch(kind, a, aoff, b, boff, 1, up, &cnt, c, d, e);
+  if (rc) return rc;
+  *count = cnt;
   return JGPM_OK;
 }
 

@@ -170,6 +170,36 @@ __device__ __forceinline__ int warp_difference(const int32_t* a, int na, const i
   return written;
 }
 
+// Splits A by B in one pass over A's keys: keys below `upper` that B lacks go to `dif`, every
+// other key of A (members of B, and keys at or above upper) to `rest` (may be null), both in
+// ascending order.  Returns |dif| (warp-uniform).  upper == INT32_MAX: no bound.  A key is
+// looked up in the part of B below upper only, where every key that can reach `dif` lies.
+// This is the one pass of both fused splits: dif_int_set (include/set_difference.cuh:346-413,
+// 415-475) is one call; fuse_set (:248-343) is one call for A \ B and A & B and one with the
+// operands swapped for B \ A.  The reference marks the hits of the second list in a zeroed
+// per-warp map to emit B \ A; a second pass of lookups needs no scratch.
+__device__ __forceinline__ int warp_split_by(const int32_t* a, int na, const int32_t* b, int nb,
+                                             int32_t upper, int32_t* dif, int32_t* rest) {
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  nb = warp_prefix_below(b, nb, upper);
+  int nd = 0, nr = 0;
+  for (int base = 0; base < na; base += 32) {
+    const int i = base + lane;
+    const bool v = i < na;
+    const int32_t key = v ? __ldg(a + i) : 0;
+    const bool f = v && (upper == INT32_MAX || key < upper) && !(nb > 0 && contains_g(b, nb, key));
+    const unsigned md = __ballot_sync(kFull, f);
+    const unsigned mr = __ballot_sync(kFull, v && !f);
+    if (f) dif[nd + __popc(md & below)] = key;
+    else if (v && rest) rest[nr + __popc(mr & below)] = key;
+    nd += __popc(md);
+    nr += __popc(mr);
+  }
+  __syncwarp();
+  return nd;
+}
+
 // Lists in shared or global memory that the warp reads with plain loads (no __ldg), for
 // operands the warp itself just wrote.
 __device__ __forceinline__ bool contains_s(const int32_t* a, int n, int32_t key) {

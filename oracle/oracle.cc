@@ -8,6 +8,7 @@
 //   * CSR construction and degree orientation: common/graph.cc:210-401 (rule at :229-230).
 //   * The scalar merge set operations of VertexSet: include/VertexSet.h:53-160 and
 //     common/VertexSet.cc:21-89 (difference excludes other.vid, the AutoMine convention).
+//   * The fused splits fuse_set and dif_int_set, include/set_difference.cuh:248-475.
 //   * The per-pattern nested-loop plans of the message-passing kernels,
 //     src/message_passing_gpu_kernels.cuh: P0 :64-102, P1 :104-186, P2 :188-252,
 //     P3 :254-334, P4 :336-420, P5 :422-502, P6 :504-576, P7 :578-659, P8 :661-745,
@@ -689,6 +690,47 @@ int orc_count_clique(int k, int32_t n, const int64_t* rowptr, const int32_t* col
 // Brute-force vertex-induced census of the six connected 4-vertex graphlets by enumerating
 // every 4-subset (tiny graphs only).  out[0..5] = 3-star, 4-path, tailed triangle, 4-cycle,
 // diamond, 4-clique.
+// fuse_set (include/set_difference.cuh:248-343): c = A \ B, d = A & B, e = B \ A of two sorted
+// lists; returns |A & B|.  As the reference's wrapper (:338-343) does, an empty A or B returns
+// 0 and writes nothing.  The reference searches the shorter list's keys in the longer one and
+// marks the hits in a map to emit the longer list's remainder; one merge gives the same sets.
+int32_t orc_fuse_set(const int32_t* a, int32_t na, const int32_t* b, int32_t nb, int32_t* c,
+                     int32_t* d, int32_t* e) {
+  if (na == 0 || nb == 0) return 0;
+  int32_t i = 0, j = 0, nc = 0, nd = 0, ne = 0;
+  while (i < na || j < nb) {
+    if (j == nb || (i < na && a[i] < b[j])) {
+      c[nc++] = a[i++];
+    } else if (i == na || b[j] < a[i]) {
+      e[ne++] = b[j++];
+    } else {
+      d[nd++] = a[i];
+      ++i;
+      ++j;
+    }
+  }
+  return nd;
+}
+
+// dif_int_set (include/set_difference.cuh:346-413): keys x of A with x < upper and x not in B
+// go to c, every other key of A to d (keys at or above upper included, the active branch at
+// :379-382); returns |c|.  upper == INT32_MAX is the unbounded form (:415-475).  An empty A or
+// B returns 0 and writes nothing (:407-413).
+int32_t orc_dif_int_set(const int32_t* a, int32_t na, const int32_t* b, int32_t nb,
+                        int32_t upper, int32_t* c, int32_t* d) {
+  if (na == 0 || nb == 0) return 0;
+  int32_t j = 0, nc = 0, nd = 0;
+  for (int32_t i = 0; i < na; ++i) {
+    const int32_t x = a[i];
+    while (j < nb && b[j] < x) ++j;
+    const bool in_b = j < nb && b[j] == x;
+    const bool below = upper == INT32_MAX || x < upper;
+    if (below && !in_b) c[nc++] = x;
+    else d[nd++] = x;
+  }
+  return nc;
+}
+
 int orc_census4(int32_t n, const int64_t* rowptr, const int32_t* col, uint64_t* out) {
   if (n > 400) return -1;
   std::vector<uint8_t> adj((size_t)n * n, 0);

@@ -48,6 +48,11 @@ def lib():
                                        _PU64, _PU64]
         L.orc_census4.restype = ctypes.c_int
         L.orc_census4.argtypes = [ctypes.c_int32, _P64, _P32, _PU64]
+        L.orc_fuse_set.restype = ctypes.c_int32
+        L.orc_fuse_set.argtypes = [_P32, ctypes.c_int32, _P32, ctypes.c_int32, _P32, _P32, _P32]
+        L.orc_dif_int_set.restype = ctypes.c_int32
+        L.orc_dif_int_set.argtypes = [_P32, ctypes.c_int32, _P32, ctypes.c_int32,
+                                      ctypes.c_int32, _P32, _P32]
         L.orc_count_embeddings.restype = ctypes.c_uint64
         L.orc_count_embeddings.argtypes = [ctypes.c_int, ctypes.c_int, _P32, ctypes.c_int32,
                                            _P64, _P32]
@@ -123,6 +128,36 @@ def census4(g):
     if rc != 0:
         raise ValueError("census4: graph too large")
     return [int(x) for x in out]
+
+
+def fuse_set(a, b):
+    """(|A & B|, A \\ B, A & B, B \\ A) as the reference's fuse_set gives them; with an empty
+    operand its count 0 and None for the unwritten lists."""
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    b = np.ascontiguousarray(b, dtype=np.int32)
+    c = np.empty(max(len(a), 1), np.int32)
+    d = np.empty(max(len(a), 1), np.int32)
+    e = np.empty(max(len(b), 1), np.int32)
+    r = int(lib().orc_fuse_set(_p(a, _P32), len(a), _p(b, _P32), len(b), _p(c, _P32),
+                               _p(d, _P32), _p(e, _P32)))
+    if len(a) == 0 or len(b) == 0:
+        return r, None, None, None
+    return r, c[: len(a) - r].copy(), d[:r].copy(), e[: len(b) - r].copy()
+
+
+def dif_int_set(a, b, upper=None):
+    """(|c|, c, d) as the reference's dif_int_set gives them (upper None: the unbounded form);
+    with an empty operand its count 0 and None for the unwritten lists."""
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    b = np.ascontiguousarray(b, dtype=np.int32)
+    up = np.iinfo(np.int32).max if upper is None else int(upper)
+    c = np.empty(max(len(a), 1), np.int32)
+    d = np.empty(max(len(a), 1), np.int32)
+    r = int(lib().orc_dif_int_set(_p(a, _P32), len(a), _p(b, _P32), len(b), up, _p(c, _P32),
+                                  _p(d, _P32)))
+    if len(a) == 0 or len(b) == 0:
+        return r, None, None
+    return r, c[:r].copy(), d[: len(a) - r].copy()
 
 
 def count_embeddings(k, edges, g):

@@ -4,6 +4,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 import jupiter_b200 as J
@@ -79,3 +80,20 @@ def test_host_rmat_edges_deterministic():
     assert len(s1) == 20000 and s1.max() < 5000 and s1.min() >= 0
     s3, _ = J.rmat_edges(5000, 20000, 0.57, 0.19, 0.19, 10)
     assert not (s1 == s3).all()
+
+
+def test_split_arguments_checked_before_the_device():
+    L = J.lib()
+    one = np.zeros(2, dtype=np.int64)
+    cnt = np.zeros(1, dtype=np.int32)
+    p64 = one.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+    p32 = cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    assert L.jgpm_setop_split_batch(7, None, p64, None, p64, 1, None, p32, None, None,
+                                    None) == -1
+    assert L.jgpm_setop_split_batch(J.SPLIT_FUSE, None, None, None, p64, 1, None, p32, None,
+                                    None, None) == -1
+    assert L.jgpm_setop_split(J.SPLIT_DIF_INT, None, -1, None, 0, 0, None, None, None,
+                              p32) == -1
+    text = open(os.path.join(ROOT, "include", "jgpm.h")).read()
+    assert re.search(rf"#define JGPM_SPLIT_FUSE {J.SPLIT_FUSE}\b", text)
+    assert re.search(rf"#define JGPM_SPLIT_DIF_INT {J.SPLIT_DIF_INT}\b", text)

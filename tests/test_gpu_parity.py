@@ -361,3 +361,97 @@ def test_setops_match_numpy(gpu):
             assert one == len(want)
         else:
             assert np.array_equal(one, want)
+
+
+def _split_pairs(rng):
+    sizes = [0, 1, 31, 32, 33, 100, 1000, 100000]
+    cases = []
+    for na in sizes:
+        for nb in sizes:
+            universe = max(4 * (na + nb), 8)
+            cases.append((np.unique(rng.integers(0, universe, na)).astype(np.int32),
+                          np.unique(rng.integers(0, universe, nb)).astype(np.int32)))
+    big = np.unique(rng.integers(0, 10**6, 200000)).astype(np.int32)
+    cases += [(big[::10000].copy(), big), (big, big[::10000].copy()), (big, big)]
+    return cases
+
+
+def test_fused_splits_match_oracle(gpu):
+    """fuse_set / dif_int_set through the C-ABI against the oracle's restatement.  Where an
+    operand is empty the reference returns 0 and writes nothing; the entry points give the
+    set algebra there (documented in the header), checked against numpy."""
+    J = gpu
+    rng = np.random.default_rng(11)
+    cases = _split_pairs(rng)
+    a_l = [c[0] for c in cases]
+    b_l = [c[1] for c in cases]
+    counts, out = J.setop_split_batch(J.SPLIT_FUSE, a_l, b_l)
+    for i, (a, b) in enumerate(cases):
+        c, d, e = out[i]
+        if len(a) and len(b):
+            r, oc, od, oe = O.fuse_set(a, b)
+        else:
+            r, oc, od, oe = 0, a, np.zeros(0, np.int32), b
+        assert counts[i] == r, (i, len(a), len(b))
+        assert np.array_equal(c, oc) and np.array_equal(d, od) and np.array_equal(e, oe), i
+    ups = np.array([np.iinfo(np.int32).max if i % 3 == 0 else
+                    int(rng.integers(0, 2 * (int(a.max(initial=1)) + 1)))
+                    for i, (a, _) in enumerate(cases)], dtype=np.int32)
+    counts, out = J.setop_split_batch(J.SPLIT_DIF_INT, a_l, b_l, upper=ups)
+    for i, (a, b) in enumerate(cases):
+        c, d, e = out[i]
+        up = None if ups[i] == np.iinfo(np.int32).max else int(ups[i])
+        if len(a) and len(b):
+            r, oc, od = O.dif_int_set(a, b, up)
+        else:
+            keep = (a < ups[i]) if up is not None else np.ones(len(a), bool)
+            r, oc, od = int(keep.sum()), a[keep], a[~keep]
+        assert counts[i] == r and e is None, (i, len(a), len(b))
+        assert np.array_equal(c, oc) and np.array_equal(d, od), i
+    # the single-pair entry point agrees with the batch
+    a, b = cases[len(cases) // 2 + 3]
+    r, c, d, e = J.setop_split(J.SPLIT_FUSE, a, b)
+    r0, oc, od, oe = O.fuse_set(a, b)
+    assert r == r0 and np.array_equal(c, oc) and np.array_equal(d, od) and np.array_equal(e, oe)
+
+
+def test_fused_split_device_arrays_and_untouched_entries(gpu):
+    """Device operands and outputs are used in place; entries the sizes leave unwritten keep
+    their contents, for host and device outputs alike."""
+    import ctypes
+    import torch
+    J = gpu
+    rng = np.random.default_rng(5)
+    a = np.unique(rng.integers(0, 5000, 1500)).astype(np.int32)
+    b = np.unique(rng.integers(0, 5000, 900)).astype(np.int32)
+    P32 = ctypes.POINTER(ctypes.c_int32)
+    P64 = ctypes.POINTER(ctypes.c_int64)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    ao = torch.tensor([0, len(a)], dtype=torch.int64, device="cuda")
+    bo = torch.tensor([0, len(b)], dtype=torch.int64, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    dc = torch.full((len(a),), -7, dtype=torch.int32, device="cuda")
+    dd = torch.full((len(a),), -7, dtype=torch.int32, device="cuda")
+    de = torch.full((len(b),), -7, dtype=torch.int32, device="cuda")
+    ptr = lambda t, p: ctypes.cast(t.data_ptr(), p)  # noqa: E731
+    rc = J.lib().jgpm_setop_split_batch(J.SPLIT_FUSE, ptr(da, P32), ptr(ao, P64), ptr(db, P32),
+                                        ptr(bo, P64), 1, None, ptr(cnt, P32), ptr(dc, P32),
+                                        ptr(dd, P32), ptr(de, P32))
+    assert rc == 0
+    torch.cuda.synchronize()
+    r, oc, od, oe = O.fuse_set(a, b)
+    assert int(cnt.item()) == r
+    c, d, e = dc.cpu().numpy(), dd.cpu().numpy(), de.cpu().numpy()
+    assert np.array_equal(c[: len(oc)], oc) and (c[len(oc):] == -7).all()
+    assert np.array_equal(d[:r], od) and (d[r:] == -7).all()
+    assert np.array_equal(e[: len(oe)], oe) and (e[len(oe):] == -7).all()
+    hc = np.full(len(a), -9, np.int32)
+    hd = np.full(len(a), -9, np.int32)
+    n = ctypes.c_int32()
+    rc = J.lib().jgpm_setop_split(J.SPLIT_DIF_INT, a.ctypes.data_as(P32), len(a),
+                                  b.ctypes.data_as(P32), len(b), 2500, hc.ctypes.data_as(P32),
+                                  hd.ctypes.data_as(P32), None, ctypes.byref(n))
+    assert rc == 0
+    r, oc, od = O.dif_int_set(a, b, 2500)
+    assert n.value == r and np.array_equal(hc[:r], oc) and (hc[r:] == -9).all()
+    assert np.array_equal(hd[: len(od)], od) and (hd[len(od):] == -9).all()

@@ -183,3 +183,39 @@ def test_rmat_generator_restatements_agree():
         s2, d2 = J.rmat_edges(n, ef * n, a, b, c, seed)
         assert np.array_equal(s1, s2) and np.array_equal(d1, d2)
         assert s1.max() < n and d1.max() < n
+
+
+def _split_cases(seed=3):
+    rng = np.random.default_rng(seed)
+    cases = []
+    for na in (0, 1, 5, 31, 32, 33, 200, 3000):
+        for nb in (0, 1, 7, 32, 65, 1000):
+            u = max(3 * (na + nb), 4)
+            cases.append((np.unique(rng.integers(0, u, na)).astype(np.int32),
+                          np.unique(rng.integers(0, u, nb)).astype(np.int32)))
+    x = np.arange(0, 500, 2, dtype=np.int32)
+    cases += [(x, x), (x, x + 1), (x[:10], x), (x, x[-3:])]
+    return cases
+
+
+def test_oracle_fused_splits_match_set_algebra():
+    """fuse_set and dif_int_set as restated: the set algebra on non-empty operands, and the
+    reference's count 0 with nothing written when an operand is empty."""
+    for i, (a, b) in enumerate(_split_cases()):
+        r, c, d, e = O.fuse_set(a, b)
+        if len(a) == 0 or len(b) == 0:
+            assert r == 0 and c is None
+        else:
+            assert r == len(np.intersect1d(a, b))
+            assert np.array_equal(c, np.setdiff1d(a, b))
+            assert np.array_equal(d, np.intersect1d(a, b))
+            assert np.array_equal(e, np.setdiff1d(b, a))
+        for up in (None, int(a[len(a) // 2]) if len(a) else 0, 0):
+            r, c, d = O.dif_int_set(a, b, up)
+            if len(a) == 0 or len(b) == 0:
+                assert r == 0 and c is None
+                continue
+            lim = np.iinfo(np.int32).max if up is None else up
+            keep = (a < lim) & ~np.isin(a, b)
+            assert r == keep.sum() and np.array_equal(c, a[keep]), (i, up)
+            assert np.array_equal(d, a[~keep]), (i, up)
