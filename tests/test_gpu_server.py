@@ -195,3 +195,31 @@ def test_light_queries_do_not_wait_behind_heavy_ones(gpu, expected):
         # submissions were microseconds apart: compare completion order through latencies
         assert max(lat for _, lat in lights) < done_heavy, (lights, done_heavy)
         assert time.perf_counter() - t0 < 60
+
+
+def test_graph_pool_split_over_two_servers(gpu, expected):
+    """The multi-GPU pool's placement and routing (jupiter_b200.pools) with two servers on one
+    device standing in for two GPUs (the servers never wait on each other): each serves the
+    queries of its own graphs, and the merged results equal the oracle for every query."""
+    from jupiter_b200 import pools
+    J = gpu
+    loads = [n * ef for n, ef, _ in SPECS]
+    owner = pools.place_graphs(loads, [16 * n * ef for n, ef, _ in SPECS], 2, 8 << 30)
+    assert sorted(set(owner.tolist())) == [0, 1]
+    rng = np.random.default_rng(2)
+    gids = rng.integers(len(SPECS), size=80)
+    pats = [PATTERNS[int(x)] for x in rng.integers(len(PATTERNS), size=80)]
+    arr = np.cumsum(rng.exponential(1e-3, 80))
+    parts = []
+    for r in range(2):
+        s = J.Server(memory_budget_bytes=8 << 30, max_inflight=3, max_batch=16)
+        with s:
+            for g in pools.local_ids(owner, r):
+                n, ef, seed = SPECS[g]
+                s.add_graph(J.Graph.rmat(n, ef, 0.57, 0.19, 0.19, seed))
+            idx, loc = pools.local_queries(gids, owner, r)
+            c, lat, wall = s.replay(loc, [pats[i] for i in idx], arr[idx])
+            parts.append((idx, c, lat, wall))
+    counts, lat, wall = pools.merge_results(len(gids), parts)
+    assert counts == [expected[(int(g), p)] for g, p in zip(gids, pats)]
+    assert not np.isnan(lat).any() and wall == max(p[3] for p in parts)
