@@ -78,6 +78,20 @@ int launch_tiers_k78(int k, int mode, const CliqueArgs& a, const TierPlan& p, in
 
 namespace {
 
+// Programmatic dependent launch between the tier kernels of one count.  The tiers share
+// nothing but their atomic result adds (each has its own cursor and its own scratch), so every
+// kernel lets the next one launch once all of its CTAs have started (tier_open), and the next
+// kernel's CTAs take the SMs that this kernel's last CTAs leave idle.  Every CTA waits at its
+// end for the previous kernel to complete (tier_close), so a kernel completes only after all
+// earlier ones, and the work queued after the last tier (the result read-back) sees every
+// tier's adds.  A kernel launched without the attribute has no such predecessor, and the wait
+// returns at once.  No wait can block a CTA that another waiter needs: a kernel launches only
+// after every CTA of its predecessor has started, so the CTAs being waited for are resident.
+__device__ __forceinline__ void tier_open() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void tier_close() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ------------------------------------------------------------------ small tiers (d <= 32)
 template <int G, int K, bool STATS, bool ETRI = false, bool PAIRS = false, bool TT = false>
 __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
@@ -89,6 +103,7 @@ __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
   const int gi = lane / G;
   uint32_t* R = rows_s + wib * 32 + gi * G;
   int* DG = deg_s + wib * 32 + gi * G;
+  tier_open();
   acc_t cnt = 0, elems = 0;
   for (;;) {
     unsigned long long c0 = 0;
@@ -109,6 +124,7 @@ __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
     if (cnt) atomicAdd(&a.ctl->count[0], cnt);
     if (STATS && elems) atomicAdd(&a.ctl->elements[0], elems);
   }
+  tier_close();
 }
 
 // ------------------------------------------------------------------ warp tier (d <= 128)
@@ -119,6 +135,7 @@ __global__ void __launch_bounds__(256, 4) k_clique_warp(CliqueArgs a) {
   extern __shared__ __align__(16) unsigned char wsmem[];
   WarpSmem& ws = reinterpret_cast<WarpSmem*>(wsmem)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
+  tier_open();
   acc_t cnt = 0, elems = 0;
   for (;;) {
     unsigned long long c0 = 0;
@@ -137,6 +154,7 @@ __global__ void __launch_bounds__(256, 4) k_clique_warp(CliqueArgs a) {
     if (cnt) atomicAdd(&a.ctl->count[0], cnt);
     if (STATS && elems) atomicAdd(&a.ctl->elements[0], elems);
   }
+  tier_close();
 }
 
 // --------------------------------------------------- CTA tiers (32 < d <= kWideMaxDeg)
@@ -161,6 +179,7 @@ __global__ void __launch_bounds__(256, kMidMinBlocks<BAL, ROWW>()) k_clique_mid(
   __shared__ unsigned long long s_idx;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
+  tier_open();
   acc_t cnt = 0, elems = 0;
   for (;;) {
     if (tid == 0) s_idx = atomicAdd(&a.ctl->counter[a.cursor], 1ull);
@@ -180,6 +199,7 @@ __global__ void __launch_bounds__(256, kMidMinBlocks<BAL, ROWW>()) k_clique_mid(
     if (cnt) atomicAdd(&a.ctl->count[0], cnt);
     if (STATS && elems) atomicAdd(&a.ctl->elements[0], elems);
   }
+  tier_close();
 }
 
 // ------------------------------------------------------------------ large tier (d > 1024)
@@ -218,6 +238,7 @@ __global__ void __launch_bounds__(256) k_clique_large(CliqueArgs a) {
   const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int32_t* buf = a.scratch + gwarp * a.scratch_per_warp;
   const int64_t cap = a.scratch_per_warp / kMaxLevels;
+  tier_open();
   acc_t cnt = 0, elems = 0;
   for (;;) {
     // task t = chunk (t mod large_chunks) of 32 arcs of root begin + t / large_chunks
@@ -272,16 +293,37 @@ __global__ void __launch_bounds__(256) k_clique_large(CliqueArgs a) {
     if (cnt) atomicAdd(&a.ctl->count[0], cnt);
     if (STATS && elems) atomicAdd(&a.ctl->elements[0], elems);
   }
+  tier_close();
 }
 
-// True (with the error recorded) if the kernel just launched failed to launch, so that a count
-// never silently misses a tier.
-inline bool launch_failed(cudaError_t* err) {
-  const cudaError_t e = cudaGetLastError();
+// True (with the error recorded) if the kernel just launched failed to launch (rc: the
+// launch call's own status), so that a count never silently misses a tier.
+inline bool launch_failed(cudaError_t* err, cudaError_t rc = cudaSuccess) {
+  const cudaError_t last = cudaGetLastError();
+  const cudaError_t e = rc != cudaSuccess ? rc : last;
   if (e == cudaSuccess) return false;
   *err = e;
   jgpm_set_error_(std::string("clique tier launch: ") + cudaGetErrorString(e));
   return true;
+}
+
+// Launches one tier kernel of 256 threads; after the first tier of a count (pdl) with
+// programmatic stream serialization, so that it overlaps the previous tier's last CTAs
+// (tier_open / tier_close).
+template <typename... Args>
+cudaError_t tier_launch(bool pdl, void (*kern)(Args...), int grid, size_t smem, cudaStream_t s,
+                        Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
 }
 
 // Register-mask width of a CTA band: k >= 7 counts warp-cooperatively (0), which keeps the
@@ -303,8 +345,8 @@ constexpr bool kBandBalanced() { return K == 5 && !STATS && !ETRI && ROWW > 0 &&
 
 template <int K, bool STATS, bool ETRI, bool PAIRS, int ROWW, int WPL = 1, bool GR = false,
           bool TT = false>
-void launch_mid_band(CliqueArgs a, const TierRange& r, int cursor, int dmax, int sms,
-                     cudaStream_t s) {
+cudaError_t launch_mid_band(CliqueArgs a, const TierRange& r, int cursor, int dmax, int sms,
+                            cudaStream_t s, bool pdl) {
   a.begin = r.b;
   a.end = r.e;
   a.step = r.step;
@@ -321,7 +363,7 @@ void launch_mid_band(CliqueArgs a, const TierRange& r, int cursor, int dmax, int
   const int64_t roots = r.e - r.b;
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, roots));
   if (GR) grid = std::min(grid, rows_band_grid(dmax, sms, roots));
-  kern<<<grid, 256, sm, s>>>(a, dmax, W);
+  return tier_launch(pdl, kern, grid, sm, s, a, dmax, W);
 }
 
 template <int K, bool STATS, bool ETRI, bool PAIRS = false, bool TT = false>
@@ -330,39 +372,45 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
   CliqueArgs a = base;
   int n = 0;
   cudaError_t err = cudaSuccess;
+  // the first tier of a count is an ordinary launch (after the control block's reset in the
+  // stream); the later ones overlap their predecessor's last CTAs
+  auto pdl = [&]() { return n > 0; };
   if (!p.large.empty()) {
     a.begin = p.large.b;
     a.end = p.large.e;
     a.step = p.large.step;
     a.cursor = 2;
-    k_clique_large<K, STATS, ETRI, PAIRS, TT><<<sms * 2, 256, 0, s>>>(a);
+    const cudaError_t rc =
+        tier_launch(pdl(), k_clique_large<K, STATS, ETRI, PAIRS, TT>, sms * 2, 0, s, a);
     ++n;
-    if (launch_failed(&err)) return -1;
+    if (launch_failed(&err, rc)) return -1;
   }
   if (!p.wide.empty()) {
-    launch_mid_band<K, STATS, ETRI, PAIRS, 0, 4, true, TT>(a, p.wide, 9,
-                                                       std::min(max_out, kWideMaxDeg), sms, s);
+    const cudaError_t rc = launch_mid_band<K, STATS, ETRI, PAIRS, 0, 4, true, TT>(
+        a, p.wide, 9, std::min(max_out, kWideMaxDeg), sms, s, pdl());
     ++n;
-    if (launch_failed(&err)) return -1;
+    if (launch_failed(&err, rc)) return -1;
   }
   if (!p.mid[0].empty()) {
-    launch_mid_band<K, STATS, ETRI, PAIRS, kWideBandRowWords<K>(), 1, false, TT>(a, p.mid[0], 1,
-                                                            std::min(max_out, kMidMaxDeg),
-                                              sms, s);
+    const cudaError_t rc =
+        launch_mid_band<K, STATS, ETRI, PAIRS, kWideBandRowWords<K>(), 1, false, TT>(
+            a, p.mid[0], 1, std::min(max_out, kMidMaxDeg), sms, s, pdl());
     ++n;
-    if (launch_failed(&err)) return -1;
+    if (launch_failed(&err, rc)) return -1;
   }
   if (!p.mid[1].empty()) {
-    launch_mid_band<K, STATS, ETRI, PAIRS, kBandRowWords<K>(16), 1, false, TT>(a, p.mid[1], 0,
-                                                                 std::min(max_out, 512), sms, s);
+    const cudaError_t rc =
+        launch_mid_band<K, STATS, ETRI, PAIRS, kBandRowWords<K>(16), 1, false, TT>(
+            a, p.mid[1], 0, std::min(max_out, 512), sms, s, pdl());
     ++n;
-    if (launch_failed(&err)) return -1;
+    if (launch_failed(&err, rc)) return -1;
   }
   if (!p.mid[2].empty()) {
-    launch_mid_band<K, STATS, ETRI, PAIRS, kBandRowWords<K>(8), 1, false, TT>(a, p.mid[2], 8,
-                                                                std::min(max_out, 256), sms, s);
+    const cudaError_t rc =
+        launch_mid_band<K, STATS, ETRI, PAIRS, kBandRowWords<K>(8), 1, false, TT>(
+            a, p.mid[2], 8, std::min(max_out, 256), sms, s, pdl());
     ++n;
-    if (launch_failed(&err)) return -1;
+    if (launch_failed(&err, rc)) return -1;
   }
   if (!p.warp.empty()) {
     a.begin = p.warp.b;
@@ -375,9 +423,10 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clique_warp<K, STATS, ETRI, PAIRS, TT>,
                                                   256, sm);
     if (per_sm < 1) per_sm = 1;
-    k_clique_warp<K, STATS, ETRI, PAIRS, TT><<<sms * per_sm, 256, sm, s>>>(a);
+    const cudaError_t rc =
+        tier_launch(pdl(), k_clique_warp<K, STATS, ETRI, PAIRS, TT>, sms * per_sm, sm, s, a);
     ++n;
-    if (launch_failed(&err)) return -1;
+    if (launch_failed(&err, rc)) return -1;
   }
   const TierRange* gr[4] = {&p.g32, &p.g16, &p.g8, &p.g4};
   for (int q = 0; q < 4; ++q) {
@@ -386,14 +435,15 @@ int launch_plan_k(const CliqueArgs& base, const TierPlan& p, int sms, cudaStream
     a.end = gr[q]->e;
     a.step = gr[q]->step;
     a.cursor = 3 + q;
+    cudaError_t rc;
     switch (q) {
-      case 0: k_clique_group<32, K, STATS, ETRI, PAIRS, TT><<<sms * 8, 256, 0, s>>>(a); break;
-      case 1: k_clique_group<16, K, STATS, ETRI, PAIRS, TT><<<sms * 8, 256, 0, s>>>(a); break;
-      case 2: k_clique_group<8, K, STATS, ETRI, PAIRS, TT><<<sms * 8, 256, 0, s>>>(a); break;
-      default: k_clique_group<4, K, STATS, ETRI, PAIRS, TT><<<sms * 8, 256, 0, s>>>(a); break;
+      case 0: rc = tier_launch(pdl(), k_clique_group<32, K, STATS, ETRI, PAIRS, TT>, sms * 8, 0, s, a); break;
+      case 1: rc = tier_launch(pdl(), k_clique_group<16, K, STATS, ETRI, PAIRS, TT>, sms * 8, 0, s, a); break;
+      case 2: rc = tier_launch(pdl(), k_clique_group<8, K, STATS, ETRI, PAIRS, TT>, sms * 8, 0, s, a); break;
+      default: rc = tier_launch(pdl(), k_clique_group<4, K, STATS, ETRI, PAIRS, TT>, sms * 8, 0, s, a); break;
     }
     ++n;
-    if (launch_failed(&err)) return -1;
+    if (launch_failed(&err, rc)) return -1;
   }
   return n;
 }
