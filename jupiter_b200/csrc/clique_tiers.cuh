@@ -78,19 +78,9 @@ int launch_tiers_k78(int k, int mode, const CliqueArgs& a, const TierPlan& p, in
 
 namespace {
 
-// Programmatic dependent launch between the tier kernels of one count.  The tiers share
-// nothing but their atomic result adds (each has its own cursor and its own scratch), so every
-// kernel lets the next one launch once all of its CTAs have started (tier_open), and the next
-// kernel's CTAs take the SMs that this kernel's last CTAs leave idle.  Every CTA waits at its
-// end for the previous kernel to complete (tier_close), so a kernel completes only after all
-// earlier ones, and the work queued after the last tier (the result read-back) sees every
-// tier's adds.  A kernel launched without the attribute has no such predecessor, and the wait
-// returns at once.  No wait can block a CTA that another waiter needs: a kernel launches only
-// after every CTA of its predecessor has started, so the CTAs being waited for are resident.
-__device__ __forceinline__ void tier_open() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-__device__ __forceinline__ void tier_close() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// The tier kernels of one count share nothing but their atomic result adds (each has its own
+// cursor and its own scratch), so every tier after the first is launched with programmatic
+// stream serialization and overlaps the previous tier's last CTAs (pdl_open / pdl_close).
 
 // ------------------------------------------------------------------ small tiers (d <= 32)
 template <int G, int K, bool STATS, bool ETRI = false, bool PAIRS = false, bool TT = false>
@@ -103,7 +93,7 @@ __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
   const int gi = lane / G;
   uint32_t* R = rows_s + wib * 32 + gi * G;
   int* DG = deg_s + wib * 32 + gi * G;
-  tier_open();
+  pdl_open();
   acc_t cnt = 0, elems = 0;
   for (;;) {
     unsigned long long c0 = 0;
@@ -124,7 +114,7 @@ __global__ void __launch_bounds__(256) k_clique_group(CliqueArgs a) {
     if (cnt) atomicAdd(&a.ctl->count[0], cnt);
     if (STATS && elems) atomicAdd(&a.ctl->elements[0], elems);
   }
-  tier_close();
+  pdl_close();
 }
 
 // ------------------------------------------------------------------ warp tier (d <= 128)
@@ -135,7 +125,7 @@ __global__ void __launch_bounds__(256, 4) k_clique_warp(CliqueArgs a) {
   extern __shared__ __align__(16) unsigned char wsmem[];
   WarpSmem& ws = reinterpret_cast<WarpSmem*>(wsmem)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  tier_open();
+  pdl_open();
   acc_t cnt = 0, elems = 0;
   for (;;) {
     unsigned long long c0 = 0;
@@ -154,7 +144,7 @@ __global__ void __launch_bounds__(256, 4) k_clique_warp(CliqueArgs a) {
     if (cnt) atomicAdd(&a.ctl->count[0], cnt);
     if (STATS && elems) atomicAdd(&a.ctl->elements[0], elems);
   }
-  tier_close();
+  pdl_close();
 }
 
 // --------------------------------------------------- CTA tiers (32 < d <= kWideMaxDeg)
@@ -179,7 +169,7 @@ __global__ void __launch_bounds__(256, kMidMinBlocks<BAL, ROWW>()) k_clique_mid(
   __shared__ unsigned long long s_idx;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  tier_open();
+  pdl_open();
   acc_t cnt = 0, elems = 0;
   for (;;) {
     if (tid == 0) s_idx = atomicAdd(&a.ctl->counter[a.cursor], 1ull);
@@ -199,7 +189,7 @@ __global__ void __launch_bounds__(256, kMidMinBlocks<BAL, ROWW>()) k_clique_mid(
     if (cnt) atomicAdd(&a.ctl->count[0], cnt);
     if (STATS && elems) atomicAdd(&a.ctl->elements[0], elems);
   }
-  tier_close();
+  pdl_close();
 }
 
 // ------------------------------------------------------------------ large tier (d > 1024)
@@ -238,7 +228,7 @@ __global__ void __launch_bounds__(256) k_clique_large(CliqueArgs a) {
   const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int32_t* buf = a.scratch + gwarp * a.scratch_per_warp;
   const int64_t cap = a.scratch_per_warp / kMaxLevels;
-  tier_open();
+  pdl_open();
   acc_t cnt = 0, elems = 0;
   for (;;) {
     // task t = chunk (t mod large_chunks) of 32 arcs of root begin + t / large_chunks
@@ -293,7 +283,7 @@ __global__ void __launch_bounds__(256) k_clique_large(CliqueArgs a) {
     if (cnt) atomicAdd(&a.ctl->count[0], cnt);
     if (STATS && elems) atomicAdd(&a.ctl->elements[0], elems);
   }
-  tier_close();
+  pdl_close();
 }
 
 // True (with the error recorded) if the kernel just launched failed to launch (rc: the
@@ -308,22 +298,11 @@ inline bool launch_failed(cudaError_t* err, cudaError_t rc = cudaSuccess) {
 }
 
 // Launches one tier kernel of 256 threads; after the first tier of a count (pdl) with
-// programmatic stream serialization, so that it overlaps the previous tier's last CTAs
-// (tier_open / tier_close).
+// programmatic stream serialization.
 template <typename... Args>
 cudaError_t tier_launch(bool pdl, void (*kern)(Args...), int grid, size_t smem, cudaStream_t s,
                         Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3(256);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = pdl ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, kern, args...);
+  return launch_pdl(pdl, kern, grid, 256, smem, s, args...);
 }
 
 // Register-mask width of a CTA band: k >= 7 counts warp-cooperatively (0), which keeps the

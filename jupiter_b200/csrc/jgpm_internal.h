@@ -115,6 +115,26 @@ struct jgpm_graph {
 void jgpm_set_error_(const std::string& msg);
 
 namespace jgpm {
+// Launches `kern`; with pdl, with programmatic stream serialization, so that it may start
+// while the previous kernel of the stream drains (the kernels pair pdl_open / pdl_close).
+template <typename... Args>
+cudaError_t launch_pdl(bool pdl, void (*kern)(Args...), int grid, int block, size_t smem,
+                       cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+}  // namespace jgpm
+
+namespace jgpm {
 // graph_build.cu
 // Device memory of graphs and their temporaries: a per-device stream-ordered pool that keeps
 // freed memory for reuse (freed memory is reused in the order of the freeing stream), so a

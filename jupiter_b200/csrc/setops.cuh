@@ -24,6 +24,18 @@ namespace jgpm {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// Programmatic dependent launch between kernels of one count that share nothing but atomic
+// result adds: pdl_open lets the next kernel (launched with programmatic stream serialization)
+// start once every CTA of this one has started, so its CTAs fill the SMs this kernel's last CTAs
+// leave idle; pdl_close, at the end of every CTA, waits for the previous kernel to complete, so
+// a kernel completes only after all earlier ones.  Without the launch attribute both are no-ops
+// in effect.  A kernel launches only after all CTAs of its predecessor have started, so the CTAs
+// a wait depends on are resident and the wait always ends.
+__device__ __forceinline__ void pdl_open() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_close() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ int lower_bound_g(const int32_t* a, int n, int32_t key) {
   int lo = 0, hi = n;
   while (lo < hi) {
