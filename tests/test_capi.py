@@ -71,6 +71,9 @@ def test_no_device_fails_loudly():
     assert e.value.code == -8  # JGPM_ENODEV
     with pytest.raises(J.JgpmError):
         J.setop(J.OP_INTERSECT_COUNT, [1, 2, 3], [2, 3])
+    with pytest.raises(J.JgpmError) as e:
+        J.setop_split(J.SPLIT_FUSE, [1, 2, 3], [2, 3])
+    assert e.value.code == -8
 
 
 def test_host_rmat_edges_deterministic():
