@@ -169,6 +169,10 @@ int jgpm_setop_batch(int op, const int32_t* a, const int64_t* a_off, const int32
     ho.resize(nops + 1);
     JGPM_CUDA_TRY(cudaMemcpy(ho.data(), out_off, (nops + 1) * 8, cudaMemcpyDefault));
   }
+  if (ha[0] < 0 || hb[0] < 0 || (ha[nops] > 0 && !a) || (hb[nops] > 0 && !b)) {
+    jgpm_set_error_("jgpm_setop_batch: bad offsets or missing operand array");
+    return JGPM_EINVAL;
+  }
   for (int64_t i = 0; i < nops; ++i) {
     const int64_t na = ha[i + 1] - ha[i], nb = hb[i + 1] - hb[i];
     if (na < 0 || nb < 0 || na > INT32_MAX || nb > INT32_MAX) {
@@ -258,8 +262,9 @@ int jgpm_setop_split_batch(int kind, const int32_t* a, const int64_t* a_off, con
     jgpm_set_error_("jgpm_setop_split_batch: bad offsets");
     return JGPM_EINVAL;
   }
-  if ((ha[nops] > 0 && (!c || !d)) || (fuse && hb[nops] > 0 && !e)) {
-    jgpm_set_error_("jgpm_setop_split_batch: missing output array");
+  if ((ha[nops] > 0 && (!a || !c || !d)) || (hb[nops] > 0 && !b) ||
+      (fuse && hb[nops] > 0 && !e)) {
+    jgpm_set_error_("jgpm_setop_split_batch: missing operand or output array");
     return JGPM_EINVAL;
   }
   for (int64_t i = 0; i < nops; ++i) {
