@@ -8,7 +8,8 @@
 //   * CSR construction and degree orientation: common/graph.cc:210-401 (rule at :229-230).
 //   * The scalar merge set operations of VertexSet: include/VertexSet.h:53-160 and
 //     common/VertexSet.cc:21-89 (difference excludes other.vid, the AutoMine convention).
-//   * The fused splits fuse_set and dif_int_set, include/set_difference.cuh:248-475.
+//   * The fused splits fuse_set and dif_int_set, include/set_difference.cuh:248-475, and the
+//     cached two-phase search they and the intersect templates use, include/search.cuh:70-203.
 //   * The per-pattern nested-loop plans of the message-passing kernels,
 //     src/message_passing_gpu_kernels.cuh: P0 :64-102, P1 :104-186, P2 :188-252,
 //     P3 :254-334, P4 :336-420, P5 :422-502, P6 :504-576, P7 :578-659, P8 :661-745,
@@ -690,6 +691,53 @@ int orc_count_clique(int k, int32_t n, const int64_t* rowptr, const int32_t* col
 // Brute-force vertex-induced census of the six connected 4-vertex graphlets by enumerating
 // every 4-subset (tiny graphs only).  out[0..5] = 3-star, 4-path, tailed triangle, 4-cycle,
 // diamond, 4-clique.
+// The reference's cached two-phase membership search, binary_search_2phase
+// (include/search.cuh:70-105), with the hit index its marking form binary_search_2phase_map
+// (:164-203) records.  A warp caches list[k * size / 32] for its 32 lanes; phase 1 bisects the
+// cache, phase 2 searches the list between the two bracketing pivots.  For each key: found[i]
+// and marked[i] (the list index the map form marks, -1 when not found).  The tests run it over
+// every key of many lists to pin that it is exact, so a plain lookup gives the same answers.
+void orc_search_2phase(const int32_t* list, int32_t size, const int32_t* keys, int64_t nkeys,
+                       uint8_t* found, int32_t* marked) {
+  constexpr int kW = 32;
+  int32_t cache[kW];
+  for (int k = 0; k < kW; ++k) cache[k] = list[(int64_t)k * size / kW];
+  for (int64_t i = 0; i < nkeys; ++i) {
+    const int32_t key = keys[i];
+    found[i] = 0;
+    marked[i] = -1;
+    int bottom = 0, top = kW, mid = 0;
+    bool hit = false;
+    while (top > bottom + 1) {
+      mid = (top + bottom) / 2;
+      const int32_t y = cache[mid];
+      if (key == y) {
+        hit = true;
+        marked[i] = (int32_t)((int64_t)mid * size / kW);
+        break;
+      }
+      if (key < y) top = mid;
+      if (key > y) bottom = mid;
+    }
+    if (!hit) {
+      int lo = (int)((int64_t)bottom * size / kW);
+      int hi = (int)((int64_t)top * size / kW) - 1;
+      while (hi >= lo) {
+        mid = (hi + lo) / 2;
+        const int32_t y = list[mid];
+        if (key == y) {
+          hit = true;
+          marked[i] = mid;
+          break;
+        }
+        if (key < y) hi = mid - 1;
+        else lo = mid + 1;
+      }
+    }
+    found[i] = hit ? 1 : 0;
+  }
+}
+
 // fuse_set (include/set_difference.cuh:248-343): c = A \ B, d = A & B, e = B \ A of two sorted
 // lists; returns |A & B|.  As the reference's wrapper (:338-343) does, an empty A or B returns
 // 0 and writes nothing.  The reference searches the shorter list's keys in the longer one and

@@ -53,6 +53,9 @@ def lib():
         L.orc_dif_int_set.restype = ctypes.c_int32
         L.orc_dif_int_set.argtypes = [_P32, ctypes.c_int32, _P32, ctypes.c_int32,
                                       ctypes.c_int32, _P32, _P32]
+        L.orc_search_2phase.restype = None
+        L.orc_search_2phase.argtypes = [_P32, ctypes.c_int32, _P32, ctypes.c_int64,
+                                        ctypes.POINTER(ctypes.c_uint8), _P32]
         L.orc_count_embeddings.restype = ctypes.c_uint64
         L.orc_count_embeddings.argtypes = [ctypes.c_int, ctypes.c_int, _P32, ctypes.c_int32,
                                            _P64, _P32]
@@ -143,6 +146,18 @@ def fuse_set(a, b):
     if len(a) == 0 or len(b) == 0:
         return r, None, None, None
     return r, c[: len(a) - r].copy(), d[:r].copy(), e[: len(b) - r].copy()
+
+
+def search_2phase(lst, keys):
+    """(found, marked index) of each key by the reference's cached two-phase search."""
+    lst = np.ascontiguousarray(lst, dtype=np.int32)
+    keys = np.ascontiguousarray(keys, dtype=np.int32)
+    found = np.zeros(len(keys), np.uint8)
+    marked = np.zeros(len(keys), np.int32)
+    lib().orc_search_2phase(_p(lst, _P32), len(lst), _p(keys, _P32), len(keys),
+                            found.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                            _p(marked, _P32))
+    return found.astype(bool), marked
 
 
 def dif_int_set(a, b, upper=None):

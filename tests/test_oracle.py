@@ -219,3 +219,20 @@ def test_oracle_fused_splits_match_set_algebra():
             keep = (a < lim) & ~np.isin(a, b)
             assert r == keep.sum() and np.array_equal(c, a[keep]), (i, up)
             assert np.array_equal(d, a[~keep]), (i, up)
+
+
+def test_reference_two_phase_search_is_exact():
+    """The reference's cached two-phase search (binary_search_2phase, and the index its map form
+    marks) finds exactly the keys a list holds, at their positions, for every list size from 1
+    to 700 and several large ones; so the plain lookups here give the same intersections and
+    differences."""
+    rng = np.random.default_rng(17)
+    sizes = list(range(1, 701)) + [1000, 1023, 1024, 1025, 4096, 100_000, 1_000_000]
+    for n in sizes:
+        lst = np.unique(rng.integers(0, 3 * n + 8, 2 * n).astype(np.int32))[:n]
+        keys = np.concatenate([lst, lst - 1, lst + 1, [lst[0] - 5, lst[-1] + 5]]).astype(np.int32)
+        found, marked = O.search_2phase(lst, keys)
+        pos = np.searchsorted(lst, keys)
+        want = (pos < len(lst)) & (lst[np.minimum(pos, len(lst) - 1)] == keys)
+        assert np.array_equal(found, want), n
+        assert np.array_equal(marked[want], pos[want]) and (marked[~want] == -1).all(), n
