@@ -9,7 +9,9 @@
 //   * The scalar merge set operations of VertexSet: include/VertexSet.h:53-160 and
 //     common/VertexSet.cc:21-89 (difference excludes other.vid, the AutoMine convention).
 //   * The fused splits fuse_set and dif_int_set, include/set_difference.cuh:248-475, and the
-//     cached two-phase search they and the intersect templates use, include/search.cuh:70-203.
+//     cached two-phase search they and the intersect templates use, with the other search
+//     variants and the hash-bin intersection, include/search.cuh:5-203 and
+//     include/operations.cuh:359-410.
 //   * The per-pattern nested-loop plans of the message-passing kernels,
 //     src/message_passing_gpu_kernels.cuh: P0 :64-102, P1 :104-186, P2 :188-252,
 //     P3 :254-334, P4 :336-420, P5 :422-502, P6 :504-576, P7 :578-659, P8 :661-745,
@@ -692,36 +694,36 @@ int orc_count_clique(int k, int32_t n, const int64_t* rowptr, const int32_t* col
 // every 4-subset (tiny graphs only).  out[0..5] = 3-star, 4-path, tailed triangle, 4-cycle,
 // diamond, 4-clique.
 // The reference's cached two-phase membership search, binary_search_2phase
-// (include/search.cuh:70-105), with the hit index its marking form binary_search_2phase_map
-// (:164-203) records.  A warp caches list[k * size / 32] for its 32 lanes; phase 1 bisects the
-// cache, phase 2 searches the list between the two bracketing pivots.  For each key: found[i]
-// and marked[i] (the list index the map form marks, -1 when not found).  The tests run it over
+// (include/search.cuh:70-105) with width 32, its CTA form binary_search_2phase_cta (:107-140)
+// with width 256, and the hit index the marking form binary_search_2phase_map (:164-203)
+// records.  The caller caches list[k * size / width] for k < width; phase 1 bisects the cache,
+// phase 2 searches the list between the two bracketing pivots.  For each key: found[i] and
+// marked[i] (the list index the map form marks, -1 when not found).  The tests run it over
 // every key of many lists to pin that it is exact, so a plain lookup gives the same answers.
-void orc_search_2phase(const int32_t* list, int32_t size, const int32_t* keys, int64_t nkeys,
-                       uint8_t* found, int32_t* marked) {
-  constexpr int kW = 32;
-  int32_t cache[kW];
-  for (int k = 0; k < kW; ++k) cache[k] = list[(int64_t)k * size / kW];
+void orc_search_2phase(const int32_t* list, int32_t size, int32_t width, const int32_t* keys,
+                       int64_t nkeys, uint8_t* found, int32_t* marked) {
+  std::vector<int32_t> cache((size_t)width);
+  for (int k = 0; k < width; ++k) cache[k] = list[(int64_t)k * size / width];
   for (int64_t i = 0; i < nkeys; ++i) {
     const int32_t key = keys[i];
     found[i] = 0;
     marked[i] = -1;
-    int bottom = 0, top = kW, mid = 0;
+    int bottom = 0, top = width, mid = 0;
     bool hit = false;
     while (top > bottom + 1) {
       mid = (top + bottom) / 2;
       const int32_t y = cache[mid];
       if (key == y) {
         hit = true;
-        marked[i] = (int32_t)((int64_t)mid * size / kW);
+        marked[i] = (int32_t)((int64_t)mid * size / width);
         break;
       }
       if (key < y) top = mid;
       if (key > y) bottom = mid;
     }
     if (!hit) {
-      int lo = (int)((int64_t)bottom * size / kW);
-      int hi = (int)((int64_t)top * size / kW) - 1;
+      int lo = (int)((int64_t)bottom * size / width);
+      int hi = (int)((int64_t)top * size / width) - 1;
       while (hi >= lo) {
         mid = (hi + lo) / 2;
         const int32_t y = list[mid];
@@ -736,6 +738,60 @@ void orc_search_2phase(const int32_t* list, int32_t size, const int32_t* keys, i
     }
     found[i] = hit ? 1 : 0;
   }
+}
+
+// binary_search_bound (include/search.cuh:142-162, unused by the reference's plans): the
+// position the search ends at for each key, as the reference computes it.
+void orc_search_bound(const int32_t* list, int32_t size, const int32_t* keys, int64_t nkeys,
+                      int32_t* pos) {
+  for (int64_t i = 0; i < nkeys; ++i) {
+    const int32_t key = keys[i];
+    int l = 0, r = size - 1, mid = 0;
+    int32_t value = 0;
+    while (r >= l) {
+      mid = l + (r - l) / 2;
+      value = list[mid];
+      if (value == key) break;
+      if (value < key) l = mid + 1;
+      else r = mid - 1;
+    }
+    pos[i] = value >= key ? mid : mid + 1;
+  }
+}
+
+// intersect_warp_hindex (include/operations.cuh:359-410, unused by the reference's plans):
+// |A & B| by hashing the shorter list into 128 bins by id mod 128 (1,024 slots each) and
+// probing every key of the longer list with a linear scan of its bin (linear_search,
+// include/search.cuh:15-29).  Returns the count, or -1 when a bin would overflow its 1,024
+// slots (the reference then writes past the bin).
+int64_t orc_hindex_count(const int32_t* a, int32_t na, const int32_t* b, int32_t nb) {
+  constexpr int kBuckets = 128, kBucketSize = 1024;
+  const int32_t* lookup = a;
+  const int32_t* search = b;
+  int32_t nl = na, ns = nb;
+  if (na > nb) {
+    lookup = b;
+    search = a;
+    nl = nb;
+    ns = na;
+  }
+  std::vector<int32_t> bins((size_t)kBuckets * kBucketSize);
+  std::vector<int32_t> count(kBuckets, 0);
+  for (int32_t i = 0; i < nl; ++i) {
+    const int32_t key = lookup[i] % kBuckets;
+    if (count[key] == kBucketSize) return -1;
+    bins[(size_t)count[key]++ * kBuckets + key] = lookup[i];
+  }
+  int64_t c = 0;
+  for (int32_t i = 0; i < ns; ++i) {
+    const int32_t v = search[i], key = v % kBuckets;
+    for (int32_t q = 0; q < count[key]; ++q)
+      if (bins[(size_t)q * kBuckets + key] == v) {
+        ++c;
+        break;
+      }
+  }
+  return c;
 }
 
 // fuse_set (include/set_difference.cuh:248-343): c = A \ B, d = A & B, e = B \ A of two sorted

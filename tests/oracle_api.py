@@ -54,8 +54,12 @@ def lib():
         L.orc_dif_int_set.argtypes = [_P32, ctypes.c_int32, _P32, ctypes.c_int32,
                                       ctypes.c_int32, _P32, _P32]
         L.orc_search_2phase.restype = None
-        L.orc_search_2phase.argtypes = [_P32, ctypes.c_int32, _P32, ctypes.c_int64,
-                                        ctypes.POINTER(ctypes.c_uint8), _P32]
+        L.orc_search_2phase.argtypes = [_P32, ctypes.c_int32, ctypes.c_int32, _P32,
+                                        ctypes.c_int64, ctypes.POINTER(ctypes.c_uint8), _P32]
+        L.orc_search_bound.restype = None
+        L.orc_search_bound.argtypes = [_P32, ctypes.c_int32, _P32, ctypes.c_int64, _P32]
+        L.orc_hindex_count.restype = ctypes.c_int64
+        L.orc_hindex_count.argtypes = [_P32, ctypes.c_int32, _P32, ctypes.c_int32]
         L.orc_count_embeddings.restype = ctypes.c_uint64
         L.orc_count_embeddings.argtypes = [ctypes.c_int, ctypes.c_int, _P32, ctypes.c_int32,
                                            _P64, _P32]
@@ -148,16 +152,33 @@ def fuse_set(a, b):
     return r, c[: len(a) - r].copy(), d[:r].copy(), e[: len(b) - r].copy()
 
 
-def search_2phase(lst, keys):
-    """(found, marked index) of each key by the reference's cached two-phase search."""
+def search_2phase(lst, keys, width=32):
+    """(found, marked index) of each key by the reference's cached two-phase search with
+    `width` pivots (32: the warp form, 256: the CTA form)."""
     lst = np.ascontiguousarray(lst, dtype=np.int32)
     keys = np.ascontiguousarray(keys, dtype=np.int32)
     found = np.zeros(len(keys), np.uint8)
     marked = np.zeros(len(keys), np.int32)
-    lib().orc_search_2phase(_p(lst, _P32), len(lst), _p(keys, _P32), len(keys),
+    lib().orc_search_2phase(_p(lst, _P32), len(lst), int(width), _p(keys, _P32), len(keys),
                             found.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
                             _p(marked, _P32))
     return found.astype(bool), marked
+
+
+def search_bound(lst, keys):
+    """The position the reference's binary_search_bound returns for each key."""
+    lst = np.ascontiguousarray(lst, dtype=np.int32)
+    keys = np.ascontiguousarray(keys, dtype=np.int32)
+    pos = np.zeros(len(keys), np.int32)
+    lib().orc_search_bound(_p(lst, _P32), len(lst), _p(keys, _P32), len(keys), _p(pos, _P32))
+    return pos
+
+
+def hindex_count(a, b):
+    """|A & B| by the reference's hash-bin intersection (-1 if a bin would overflow)."""
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    b = np.ascontiguousarray(b, dtype=np.int32)
+    return int(lib().orc_hindex_count(_p(a, _P32), len(a), _p(b, _P32), len(b)))
 
 
 def dif_int_set(a, b, upper=None):

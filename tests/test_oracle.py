@@ -221,18 +221,31 @@ def test_oracle_fused_splits_match_set_algebra():
             assert np.array_equal(d, a[~keep]), (i, up)
 
 
-def test_reference_two_phase_search_is_exact():
-    """The reference's cached two-phase search (binary_search_2phase, and the index its map form
-    marks) finds exactly the keys a list holds, at their positions, for every list size from 1
-    to 700 and several large ones; so the plain lookups here give the same intersections and
-    differences."""
+def test_reference_search_variants_are_exact():
+    """The reference's search variants, restated, against a plain lookup: the cached two-phase
+    search with 32 pivots (warp) and 256 (CTA) finds exactly the keys a list holds, at their
+    positions (the index the map form marks), for every list size from 1 to 700 and several
+    large ones; binary_search_bound is the lower bound on non-empty lists; the hash-bin
+    intersection counts |A & B| while no bin overflows.  So the plain lookups here (binary
+    lifting, merge path) give the same intersections and differences."""
     rng = np.random.default_rng(17)
     sizes = list(range(1, 701)) + [1000, 1023, 1024, 1025, 4096, 100_000, 1_000_000]
     for n in sizes:
         lst = np.unique(rng.integers(0, 3 * n + 8, 2 * n).astype(np.int32))[:n]
         keys = np.concatenate([lst, lst - 1, lst + 1, [lst[0] - 5, lst[-1] + 5]]).astype(np.int32)
-        found, marked = O.search_2phase(lst, keys)
         pos = np.searchsorted(lst, keys)
         want = (pos < len(lst)) & (lst[np.minimum(pos, len(lst) - 1)] == keys)
-        assert np.array_equal(found, want), n
-        assert np.array_equal(marked[want], pos[want]) and (marked[~want] == -1).all(), n
+        for width in (32, 256):
+            found, marked = O.search_2phase(lst, keys, width)
+            assert np.array_equal(found, want), (n, width)
+            assert np.array_equal(marked[want], pos[want]) and (marked[~want] == -1).all(), n
+        assert np.array_equal(O.search_bound(lst, keys), pos), n
+    # on an empty list binary_search_bound returns 1 for a positive key, not 0
+    assert list(O.search_bound(np.zeros(0, np.int32), [5, 0, -3])) == [1, 0, 0]
+    for na, nb in ((0, 10), (1, 1), (50, 3000), (3000, 50), (20000, 20000), (100000, 7)):
+        a = np.unique(rng.integers(0, 4 * (na + nb) + 8, na)).astype(np.int32)
+        b = np.unique(rng.integers(0, 4 * (na + nb) + 8, nb)).astype(np.int32)
+        assert O.hindex_count(a, b) == len(np.intersect1d(a, b)), (na, nb)
+    # more than 1,024 keys of one residue mod 128 overflow a bin
+    assert O.hindex_count(np.arange(0, 128 * 1100, 128, dtype=np.int32),
+                          np.arange(0, 128 * 1200, 128, dtype=np.int32)) == -1
