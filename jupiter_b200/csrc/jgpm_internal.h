@@ -132,9 +132,7 @@ cudaError_t launch_pdl(bool pdl, void (*kern)(Args...), int grid, int block, siz
   cfg.numAttrs = pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, args...);
 }
-}  // namespace jgpm
 
-namespace jgpm {
 // graph_build.cu
 // Device memory of graphs and their temporaries: a per-device stream-ordered pool that keeps
 // freed memory for reuse (freed memory is reused in the order of the freeing stream), so a
