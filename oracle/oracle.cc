@@ -740,6 +740,35 @@ void orc_search_2phase(const int32_t* list, int32_t size, int32_t width, const i
   }
 }
 
+// count_smaller (include/operations.cuh:80-124), the rank of `bound` in a sorted list as P2
+// and P9 use it (src/message_passing_gpu_kernels.cuh:241, 815), for one warp: lane 0 narrows
+// [begin, end) while it spans more than 128 elements (returning mid on a hit, and moving end to
+// mid - 1 on a miss above), then the warp counts the elements below the bound 32 at a time until
+// a chunk is not all below.
+uint32_t orc_count_smaller(int32_t bound, const int32_t* a, int32_t size) {
+  if (size == 0) return 0;
+  unsigned begin = 0, end = (unsigned)size;
+  int l = 0, r = size, mid = 0;
+  while (r - l > 32 * 4) {
+    mid = l + (r - l) / 2;
+    const int32_t value = a[mid];
+    if (value == bound) return (uint32_t)mid;
+    if (value < bound) begin = mid + 1;
+    else end = mid - 1;
+    l = (int)begin;
+    r = (int)end;
+  }
+  unsigned count = begin;
+  for (int base = l; base < r; base += 32) {
+    const int lanes = std::min(32, r - base);
+    unsigned below = 0;
+    for (int q = 0; q < lanes; ++q) below += a[base + q] < bound ? 1u : 0u;
+    count += below;
+    if (below != 32u) break;  // the ballot is not the full mask
+  }
+  return count;
+}
+
 // binary_search_bound (include/search.cuh:142-162, unused by the reference's plans): the
 // position the search ends at for each key, as the reference computes it.
 void orc_search_bound(const int32_t* list, int32_t size, const int32_t* keys, int64_t nkeys,

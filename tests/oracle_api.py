@@ -56,6 +56,8 @@ def lib():
         L.orc_search_2phase.restype = None
         L.orc_search_2phase.argtypes = [_P32, ctypes.c_int32, ctypes.c_int32, _P32,
                                         ctypes.c_int64, ctypes.POINTER(ctypes.c_uint8), _P32]
+        L.orc_count_smaller.restype = ctypes.c_uint32
+        L.orc_count_smaller.argtypes = [ctypes.c_int32, _P32, ctypes.c_int32]
         L.orc_search_bound.restype = None
         L.orc_search_bound.argtypes = [_P32, ctypes.c_int32, _P32, ctypes.c_int64, _P32]
         L.orc_hindex_count.restype = ctypes.c_int64
@@ -163,6 +165,12 @@ def search_2phase(lst, keys, width=32):
                             found.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
                             _p(marked, _P32))
     return found.astype(bool), marked
+
+
+def count_smaller(bound, lst):
+    """The reference's count_smaller(bound, list) as it computes it."""
+    lst = np.ascontiguousarray(lst, dtype=np.int32)
+    return int(lib().orc_count_smaller(int(bound), _p(lst, _P32), len(lst)))
 
 
 def search_bound(lst, keys):

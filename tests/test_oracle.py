@@ -249,3 +249,21 @@ def test_reference_search_variants_are_exact():
     # more than 1,024 keys of one residue mod 128 overflow a bin
     assert O.hindex_count(np.arange(0, 128 * 1100, 128, dtype=np.int32),
                           np.arange(0, 128 * 1200, 128, dtype=np.int32)) == -1
+
+
+def test_reference_count_smaller_is_exact_for_member_bounds():
+    """The reference's count_smaller, restated: for a bound in the list it is the bound's rank, so
+    the P2/P9 sum over every member of W is |W| (|W| - 1) / 2, the closed form the plans here
+    use; for bounds not in the list its narrowing step (end = mid - 1) can miss one element."""
+    rng = np.random.default_rng(23)
+    off_by_one = 0
+    for n in list(range(1, 400)) + [513, 1000, 2048, 5000]:
+        w = np.unique(rng.integers(0, 3 * n + 8, 2 * n).astype(np.int32))[:n]
+        ranks = [O.count_smaller(int(x), w) for x in w]
+        assert ranks == list(range(len(w))), n
+        assert sum(ranks) == len(w) * (len(w) - 1) // 2
+        for x in rng.integers(-1, 3 * n + 9, 8):
+            got, want = O.count_smaller(int(x), w), int(np.searchsorted(w, x))
+            assert got in (want, want - 1), (n, x)
+            off_by_one += got != want
+    assert off_by_one > 0  # the quirk for bounds outside the list is real
