@@ -100,3 +100,24 @@ def test_split_arguments_checked_before_the_device():
     text = open(os.path.join(ROOT, "include", "jgpm.h")).read()
     assert re.search(rf"#define JGPM_SPLIT_FUSE {J.SPLIT_FUSE}\b", text)
     assert re.search(rf"#define JGPM_SPLIT_DIF_INT {J.SPLIT_DIF_INT}\b", text)
+
+
+def test_cli_usage_and_loud_failure_without_a_device(tmp_path):
+    """The reference CLI's counterpart: usage on no arguments, and a status message with a
+    non-zero exit when there is no device (no CPU fallback)."""
+    import subprocess
+    import sys
+    cli = os.path.join(ROOT, "jupiter_b200", "jupiter_gpm")
+    assert os.path.exists(cli)
+    r = subprocess.run([cli], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Usage:" in r.stdout and "[pattern(P1)]" in r.stdout
+    if J.device_count() > 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    g = O.rmat_graph(500, 4, 0.57, 0.19, 0.19, 3)
+    prefix = str(tmp_path / "graph")
+    O.write_reference_files(g, prefix)
+    r = subprocess.run([cli, prefix, "P1"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "status -8" in (r.stdout + r.stderr)
+    assert "gpu count" not in r.stdout
