@@ -337,7 +337,7 @@ int jgpm_server_destroy(jgpm_server* s);
  * 96-102, 163-170, 239-245) and the VertexSet operators (include/VertexSet.h:53-160).
  * Note: the reference's difference_num returns 0 when B is empty
  * (include/set_difference.cuh:44-45); this entry point returns |A'| as the set algebra
- * says. */
+ * says, and as the reference's own bool-flag overload of difference_num does (:506-520). */
 int jgpm_setop(int op, const int32_t* a, int32_t na, const int32_t* b, int32_t nb,
                int32_t upper, int32_t exclude, int32_t* out, int32_t* out_n);
 
