@@ -73,12 +73,16 @@ typedef struct {
 #define JGPM_COUNT_FORCE_ENUM 4u     /* vertex-induced patterns: enumerate with set difference */
 
 /* ---- library --------------------------------------------------------------------- */
+/* The library's version string, naming its sm_100a build.  No reference counterpart. */
 const char* jgpm_version(void);
-/* Message of the calling thread's last failed call ("" if none). */
+/* Message of the calling thread's last failed call ("" if none).  Replaces the reference's
+ * print-and-exit error handling (CUDA_SAFE_CALL, include/cutil_subset.h:4-16). */
 const char* jgpm_last_error(void);
-/* Number of visible CUDA devices. */
+/* Number of visible CUDA devices; replaces cudaGetDeviceCount in SubgraphSolver
+ * (src/jupiter_gpm.cu:33). */
 int jgpm_device_count(int* n);
-/* Selects the device used by graphs created afterwards on this thread. */
+/* Selects the device used by graphs created afterwards on this thread; replaces the per-rank
+ * cudaSetDevice (src/jupiter_gpm.cu:53, 310). */
 int jgpm_set_device(int device);
 
 /* ---- graphs ---------------------------------------------------------------------- */
@@ -96,8 +100,8 @@ int jgpm_graph_from_csr(const int64_t* rowptr, const int32_t* col, int32_t n, in
                         int orient_dag, jgpm_graph** g);
 
 /* Builds a graph from an undirected host edge list: both directions are added, self-loops
- * dropped, rows sorted and deduplicated on the device.  (The reference reads prebuilt CSRs
- * only; this is the ingest step before its loader.) */
+ * dropped, rows sorted and deduplicated on the device.  No reference counterpart (the
+ * reference reads prebuilt CSRs only; this is the ingest step before its loader). */
 int jgpm_graph_from_edges(const int32_t* src, const int32_t* dst, int64_t num_edges,
                           int32_t n, int orient_dag, jgpm_graph** g);
 
@@ -109,20 +113,26 @@ int jgpm_graph_rmat(int64_t n, int64_t num_edges, double a, double b, double c, 
                     int orient_dag, jgpm_graph** g);
 
 /* The same seeded R-MAT edges on the host (no GPU needed): writes up to num_edges pairs and
- * the number written (edges with no valid draw in 64 attempts are dropped). */
+ * the number written (edges with no valid draw in 64 attempts are dropped).  No reference
+ * counterpart. */
 int jgpm_rmat_edges(int64_t n, int64_t num_edges, double a, double b, double c, uint64_t seed,
                     int32_t* src, int32_t* dst, int64_t* out_count);
 
+/* Sizes and degrees of a graph: Graph::num_vertices / num_edges / get_max_degree
+ * (include/graph.h:50-59). */
 int jgpm_graph_get_info(const jgpm_graph* g, jgpm_graph_info* info);
 
 /* Copies the symmetric CSR (dag=0) or the DAG (dag=1, built if needed) to host arrays of
- * n+1 and num_arcs / num_dag_arcs entries. */
+ * n+1 and num_arcs / num_dag_arcs entries: Graph::out_rowptr / out_colidx
+ * (include/graph.h:69-70). */
 int jgpm_graph_copy_csr(jgpm_graph* g, int dag, int64_t* rowptr, int32_t* col);
 
 /* Writes the symmetric CSR (dag=0) or the DAG (dag=1) in the reference's on-disk format.
  * Replaces Graph::dump_binary (common/graph.cc:727-753). */
 int jgpm_graph_save(jgpm_graph* g, const char* prefix, int dag);
 
+/* Releases the handle and its device memory: Graph::~Graph (include/graph.h:45) and the
+ * device CSR's teardown. */
 void jgpm_graph_free(jgpm_graph* g);
 
 /* The CUDA stream (a cudaStream_t, as an opaque pointer) on which every kernel of this graph
@@ -145,7 +155,8 @@ int jgpm_graph_stream(jgpm_graph* g, void** stream);
 int jgpm_count(jgpm_graph* g, const char* pattern, int induced, int chunk_size, uint64_t* out,
                jgpm_stats* st);
 
-/* jgpm_count with JGPM_COUNT_* flags. */
+/* jgpm_count with JGPM_COUNT_* flags (the same reference interface,
+ * src/jupiter_gpm.cu:356-375, 393-428, 873-908). */
 int jgpm_count_ex(jgpm_graph* g, const char* pattern, int induced, int chunk_size,
                   unsigned flags, uint64_t* out, jgpm_stats* st);
 
@@ -206,7 +217,8 @@ int jgpm_list(jgpm_graph* g, const char* pattern, int induced, int32_t* out, int
               int64_t* total, jgpm_stats* st);
 
 /* Vertex-induced census of the six connected 4-vertex graphlets, out[0..5] = 3-star,
- * 4-path, tailed triangle, 4-cycle, diamond, 4-clique. */
+ * 4-path, tailed triangle, 4-cycle, diamond, 4-clique.  No reference counterpart (the
+ * reference has no vertex-induced plans). */
 int jgpm_census4(jgpm_graph* g, uint64_t out[6], jgpm_stats* st);
 
 /* ---- batched counting -------------------------------------------------------------- */
@@ -252,12 +264,16 @@ typedef struct {
  * Replaces, for a whole batch, the reference's per-query round loop and static chunking
  * (src/jupiter_gpm.cu:356-375).  tuning = NULL uses the defaults.  All graphs must be on one
  * device. */
+/* Counts every job of `jobs` in one batched launch (one to three persistent kernels) and
+ * writes counts[i] for job i.  Replaces one SubgraphSolver run per (graph, pattern)
+ * (src/jupiter_gpm.cu:356-428) with its root-edge task queue in place of chunk_size's static
+ * slices (:373-377). */
 int jgpm_batch_count(const jgpm_job* jobs, int32_t njobs, const jgpm_tuning* tuning,
                      uint64_t* counts, jgpm_batch_stats* st);
 
 /* Sets the lane-group and split knobs (min_group, split_degree) the plain clique kernels of
  * this graph use; split_degree in {32, 64, 128} (roots of out-degree 32 < d <= split run one per
- * warp, larger ones one per CTA).  Counts do not depend on it. */
+ * warp, larger ones one per CTA).  Counts do not depend on it.  No reference counterpart. */
 int jgpm_graph_set_tuning(jgpm_graph* g, const jgpm_tuning* tuning);
 
 /* Picks the tuning by timing candidate settings (coordinate descent over the four knobs) on
@@ -287,11 +303,14 @@ typedef struct {
   double mean_batch;            /* queries per batch */
 } jgpm_server_stats;
 
+/* Starts a server (its scheduler thread, slots and plain lanes) on cfg->device.  No reference
+ * counterpart. */
 int jgpm_server_create(const jgpm_server_config* cfg, jgpm_server** s);
 
 /* Adds a graph to the pool; the server takes ownership of the handle (it frees it in
  * jgpm_server_destroy).  The graph's DAG and root tiers are built now.  Evicted graphs keep a
- * host copy and are uploaded again on demand (least recently used graphs go first). */
+ * host copy and are uploaded again on demand (least recently used graphs go first).  No
+ * reference counterpart. */
 int jgpm_server_add_graph(jgpm_server* s, jgpm_graph* g, int32_t* graph_id);
 
 /* Queues a counting query and returns its ticket at once.  Batchable patterns (see jgpm_job)
@@ -303,24 +322,30 @@ int jgpm_server_add_graph(jgpm_server* s, jgpm_graph* g, int32_t* graph_id);
  * shortest estimated work first, with aging: the estimate is the running average of the
  * service times measured for the same (graph, pattern) (before the first, a prior from the
  * graph's DAG arcs and the pattern), less 0.1 s per second the query has waited, so light
- * queries do not wait behind heavy ones and no query waits for ever. */
+ * queries do not wait behind heavy ones and no query waits for ever.  No reference
+ * counterpart. */
 int jgpm_server_submit(jgpm_server* s, int32_t graph_id, const char* pattern, uint64_t* ticket);
 
-/* Waits up to timeout_ms (< 0: no limit) for a ticket; JGPM_ETIMEDOUT if it is not done. */
+/* Waits up to timeout_ms (< 0: no limit) for a ticket; JGPM_ETIMEDOUT if it is not done.
+ * No reference counterpart. */
 int jgpm_server_wait(jgpm_server* s, uint64_t ticket, int32_t timeout_ms, uint64_t* count,
                      double* latency_ms);
 
+/* Query, batch and pool counters since the server started.  No reference counterpart. */
 int jgpm_server_get_stats(jgpm_server* s, jgpm_server_stats* st);
 
 /* Replays an open-loop trace: query i (graph_ids[i], patterns[i]) is submitted at
  * arrival_s[i] seconds after the start, from a generator thread inside the library.
  * mode 0 = through the server (continuous batching); mode 1 = each query as its own plain
  * jgpm_count call, served one at a time in arrival order.  Fills counts[i] and
- * latency_ms[i] (completion - arrival) and the wall time of the whole replay. */
+ * latency_ms[i] (completion - arrival) and the wall time of the whole replay.  No reference
+ * counterpart. */
 int jgpm_server_replay(jgpm_server* s, int32_t mode, int64_t n, const int32_t* graph_ids,
                        const char* const* patterns, const double* arrival_s, uint64_t* counts,
                        double* latency_ms, double* wall_s);
 
+/* Stops the server: its threads exit, the batches already on the device complete, queries
+ * not yet launched are dropped, and its graphs are freed.  No reference counterpart. */
 int jgpm_server_destroy(jgpm_server* s);
 
 /* ---- set operations -------------------------------------------------------------- */
@@ -341,7 +366,9 @@ int jgpm_server_destroy(jgpm_server* s);
 int jgpm_setop(int op, const int32_t* a, int32_t na, const int32_t* b, int32_t nb,
                int32_t upper, int32_t exclude, int32_t* out, int32_t* out_n);
 
-/* A batch of set operations in one launch: pair i is A = a[a_off[i] .. a_off[i+1]) and
+/* A batch of set operations in one launch (the templates jgpm_setop replaces,
+ * include/set_intersect.cuh and include/set_difference.cuh, one warp per pair): pair i is
+ * A = a[a_off[i] .. a_off[i+1]) and
  * B = b[b_off[i] .. b_off[i+1]), with per-pair bounds (upper/exclude arrays may be NULL).
  * Counts go to counts[i]; for the materialising ops results go to out[out_off[i] ..) where
  * out_off (nops+1 entries, host) gives each pair's capacity.  Host or device arrays. */
@@ -367,7 +394,8 @@ int jgpm_setop_batch(int op, const int32_t* a, const int64_t* a_off, const int32
 int jgpm_setop_split(int kind, const int32_t* a, int32_t na, const int32_t* b, int32_t nb,
                      int32_t upper, int32_t* c, int32_t* d, int32_t* e, int32_t* count);
 
-/* A batch of fused splits in one launch (one warp per pair), pairs given by offsets as in
+/* A batch of fused splits in one launch (fuse_set / dif_int_set,
+ * include/set_difference.cuh:248-475, one warp per pair), pairs given by offsets as in
  * jgpm_setop_batch.  Pair i writes c[a_off[i] ..) and d[a_off[i] ..) (arrays of a_off[nops]
  * entries) and e[b_off[i] ..) (b_off[nops] entries): the outputs are laid out like the
  * inputs.  upper may be NULL (no bounds).  Host or device arrays. */

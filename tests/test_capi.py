@@ -121,3 +121,20 @@ def test_cli_usage_and_loud_failure_without_a_device(tmp_path):
     r = subprocess.run([cli, prefix, "P1"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "status -8" in (r.stdout + r.stderr)
     assert "gpu count" not in r.stdout
+
+
+def test_every_entry_point_cites_its_reference_interface():
+    """Each declaration in include/*.h is preceded by a comment that cites the reference file
+    it replaces (path, usually with lines) or says it has no reference counterpart."""
+    pat = re.compile(r"(/\*(?:(?!\*/).)*\*/\s*)?((?:#define[^\n]*\n\s*)*)(?:const\s+)?"
+                     r"[A-Za-z_][A-Za-z0-9_]*\s*\**\s*(jgpm_[A-Za-z0-9_]+)\s*\(", re.S)
+    missing, seen = [], 0
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if not h.endswith(".h"):
+            continue
+        for m in pat.finditer(open(os.path.join(ROOT, "include", h)).read()):
+            seen += 1
+            c = m.group(1) or ""
+            if not (re.search(r"[A-Za-z_/]+\.(cc|cu|cuh|h|mk)\b", c) or "counterpart" in c.lower()):
+                missing.append(m.group(3))
+    assert seen >= 30 and not missing, missing
